@@ -1,0 +1,133 @@
+/*
+ * ogx.h -- C ABI of the B200 adaptive-FMM force library (libogx.so).
+ *
+ * Drop-in boundary for on-galaxy's galaxy3d::ForceSolver3D
+ * (src3d/ForceSolver3D.hpp:20-28):
+ *     virtual Accelerations3D computeAccelerations(const Bodies3D&) const = 0;
+ *     virtual const char* name() const = 0;
+ * A std::vector<Vec3> is contiguous x,y,z doubles, so Bodies3D::pos.data()
+ * and Bodies3D::mass.data() pass straight through as `pos` / `mass` below,
+ * and the returned accelerations land in a std::vector<Vec3> the same way.
+ *
+ * Conventions shared by every entry point:
+ *   - return value: OGX_OK (0) or an ogx_status error code; no exceptions,
+ *     no exit() across the ABI; ogx_strerror() names the code.
+ *   - positions/accelerations: n x 3 doubles (x,y,z per body), original order.
+ *   - potentials: n doubles, pot_i = -G * sum_{j!=i} m_j / sqrt(r_ij^2 + eps^2)
+ *     (direct) or its FMM approximation; NULL skips the potential.
+ *   - a handle is not thread-safe: one handle per host thread / stream.
+ *   - all device work is issued on the handle's stream.
+ */
+#ifndef OGX_H
+#define OGX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    OGX_OK = 0,
+    OGX_ERR_INVALID = 1,      /* bad argument (n, p, leaf capacity, pointers) */
+    OGX_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    OGX_ERR_NO_DEVICE = 3,    /* no usable CUDA device */
+    OGX_ERR_OOM = 4,          /* device allocation failed or over budget */
+    OGX_ERR_UNSUPPORTED = 5,  /* valid request this build cannot serve */
+    OGX_ERR_TIMEOUT = 6,      /* a bounded device wait ran out */
+    OGX_ERR_STATE = 7         /* call out of sequence (e.g. step before upload) */
+} ogx_status;
+
+typedef enum {
+    OGX_SOLVER_ADAPTIVE_FMM = 0, /* replaces AdaptiveFMM3D (src3d/AdaptiveFMM3D.hpp:20) */
+    OGX_SOLVER_DIRECT = 1        /* replaces DirectSolver3D (src3d/DirectSolver3D.hpp:11) */
+} ogx_solver;
+
+typedef enum {
+    OGX_PREC_FP64 = 0,  /* plain form: FP64 end to end, matches AdaptiveFMM3D to <=1e-12 */
+    OGX_PREC_MIXED = 1  /* FP32 P2P + split-precision tensor-core M2L, FP64 upper translations */
+} ogx_precision;
+
+typedef struct {
+    double G;            /* gravitational constant (KernelParams3D::G) */
+    double eps;          /* Plummer softening (KernelParams3D::eps); also the leaf-edge floor */
+    int p;               /* expansion order, 1..12 (AdaptiveFMM3D p) */
+    int leaf_capacity;   /* split threshold (AdaptiveFMM3D threshold), >= 1 */
+    int solver;          /* ogx_solver */
+    int precision;       /* ogx_precision */
+    int device;          /* CUDA device ordinal */
+    void* stream;        /* cudaStream_t to issue on; NULL = a stream owned by the handle */
+} ogx_params;
+
+typedef struct {
+    int64_t n;                 /* bodies in the last evaluation */
+    int32_t num_boxes;         /* AdaptiveFMM3D::lastNumBoxes */
+    int32_t num_leaves;
+    int32_t max_leaf_occupancy;/* AdaptiveFMM3D::lastMaxLeafOcc */
+    int32_t max_level;
+    int64_t list_u, list_v, list_w, list_x; /* interaction-list sizes (pairs of boxes) */
+    int64_t p2p_pairs;         /* body-body interactions of the U lists (incl. none for self) */
+    int64_t m2p_evals;         /* body x W-box evaluations */
+    int64_t p2l_evals;         /* source-body x X-box evaluations */
+    int64_t adjacency_mismatch;/* integer vs FP64 adjacency disagreements (0 expected) */
+    double ms_tree, ms_lists, ms_upward, ms_m2l, ms_p2l, ms_downward, ms_leaf, ms_total;
+    double ms_h2d, ms_d2h;     /* host-buffer calls only */
+} ogx_stats;
+
+/* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0. */
+int ogx_params_default(ogx_params* prm);
+
+/* Constructor: AdaptiveFMM3D(KernelParams3D, int p, int threshold) (src3d/AdaptiveFMM3D.hpp:22-23)
+ * or DirectSolver3D(KernelParams3D) (src3d/DirectSolver3D.hpp:13). */
+int ogx_create(const ogx_params* prm, void** handle);
+int ogx_destroy(void* handle);
+
+/* ForceSolver3D::computeAccelerations (src3d/ForceSolver3D.hpp:24) with HOST buffers:
+ * copies in, evaluates, copies out, synchronises.  pot may be NULL. */
+int ogx_eval(void* handle, int64_t n, const double* pos, const double* mass, double* acc, double* pot);
+
+/* Same evaluation on DEVICE buffers (pos n*3, mass n, acc n*3, pot n or NULL), issued on the
+ * handle's stream.  Returns after the work is enqueued; the tree sizes are read back once per
+ * call so the host knows the launch shapes.  Call ogx_synchronize() before reading acc. */
+int ogx_eval_device(void* handle, int64_t n, const double* d_pos, const double* d_mass, double* d_acc,
+                    double* d_pot);
+int ogx_synchronize(void* handle);
+
+/* ForceSolver3D::name (src3d/ForceSolver3D.hpp:26). */
+const char* ogx_name(void* handle);
+int ogx_last_stats(void* handle, ogx_stats* out);
+const char* ogx_strerror(int status);
+/* Text of the last error raised on the calling host thread (CUDA message etc.). */
+const char* ogx_last_error_message(void);
+/* Host-only helper (no GPU needed): the level-independent translation matrix used by the
+ * kernels, K x K row-major with K=(p+1)^2 over the real coefficient layout
+ * dof(n,0)=n^2, dof(n,m>0)=n^2+2m-1 (re) / n^2+2m (im), scaled M'=M/side^n, L'=L*side^n.
+ * kind 0: M2M child octant index (0..7); 1: L2L child octant index (0..7);
+ * 2: M2L source-minus-target offset index (ox+3)+7(oy+3)+49(oz+3) (0..342).
+ * Replaces the per-pair operators fmm::M2M / fmm::L2L / fmm::M2L
+ * (src3d/FmmExpansions3D.hpp:242-330). */
+int ogx_operator_matrix(int kind, int p, int index, double* out);
+
+/* ---- device-resident leapfrog: VelocityVerlet3D (src3d/Integrator3D.hpp:15-47) ----
+ * upload = bodies onto the device + initialize() (one force evaluation);
+ * step   = drift x += v dt + a dt^2/2, evaluate, kick v += (a_old + a_new) dt/2;
+ * download copies pos/vel/acc (any may be NULL) back to the host. */
+int ogx_upload(void* handle, int64_t n, const double* pos, const double* vel, const double* mass);
+int ogx_step(void* handle, double dt, int nsteps);
+int ogx_download(void* handle, double* pos, double* vel, double* acc);
+
+/* ---- tree export of the last adaptive evaluation (parity tests) ----
+ * sizes[0]=boxes [1]=leaves [2..6]=|colleague|,|U|,|V|,|W|,|X| (AdaptiveOctree::buildLists,
+ * src3d/AdaptiveOctree.hpp:137-189).
+ * boxes: num_boxes x 8 int32 (level, ix, iy, iz, parent, leaf, pfirst, pcount),
+ * centers: num_boxes x 4 doubles (cx, cy, cz, half), perm: sorted position -> original index.
+ * which: 0=colleague 1=U 2=V 3=W 4=X; off has num_boxes+1 entries. */
+int ogx_tree_sizes(void* handle, int64_t* sizes);
+int ogx_tree_boxes(void* handle, int32_t* boxes, double* centers, int32_t* perm);
+int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OGX_H */

@@ -1,0 +1,548 @@
+// ogx_api.cu -- the C ABI (include/ogx.h) and the host runtime behind it.
+//
+// One handle = one solver instance on one device and stream, the C-level
+// equivalent of constructing AdaptiveFMM3D / DirectSolver3D
+// (src3d/AdaptiveFMM3D.hpp:22-23, src3d/DirectSolver3D.hpp:13).  The handle
+// owns a grow-only arena of device buffers (reused across evaluations, so a
+// steady-state step allocates nothing), pinned host buffers for the two
+// per-evaluation read-backs of tree sizes, the level-independent operator
+// matrices of its expansion order, and the device-resident integrator state.
+// Errors are status codes; nothing throws or exits across the boundary
+// (the reference exit()s on CUDA errors, src3d/gpu/AdaptiveFMM3DGPU.cu:23-26).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "ogx_harmonics.cuh"
+
+namespace ogx {
+
+static thread_local std::string g_last_error;
+void set_last_error(int, const std::string& msg) { g_last_error = msg; }
+
+int Arena::get(Slot s, size_t bytes, void** out) {
+    if (cap[s] < bytes) {
+        if (ptr[s]) {
+            cudaFree(ptr[s]);
+            total -= cap[s];
+            ptr[s] = nullptr;
+            cap[s] = 0;
+        }
+        size_t nb = bytes + bytes / 4;
+        nb = (nb + 255) & ~(size_t)255;
+        const cudaError_t e = cudaMalloc(&ptr[s], nb);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ptr[s] = nullptr;
+            set_last_error(OGX_ERR_OOM, "device allocation failed");
+            return OGX_ERR_OOM;
+        }
+        cap[s] = nb;
+        total += nb;
+    }
+    *out = ptr[s];
+    return OGX_OK;
+}
+
+void Arena::release() {
+    for (int s = 0; s < S_NUM_SLOTS; ++s) {
+        if (ptr[s]) cudaFree(ptr[s]);
+        ptr[s] = nullptr;
+        cap[s] = 0;
+    }
+    total = 0;
+}
+
+// ---- operator tables: built once per order in this process, transposed k-major ----
+struct HostOps {
+    std::vector<double> m2l, m2m, l2l;
+};
+static std::mutex g_ops_mu;
+static std::map<int, std::shared_ptr<HostOps>> g_ops;
+
+static std::shared_ptr<HostOps> host_ops(int p) {
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    auto it = g_ops.find(p);
+    if (it != g_ops.end()) return it->second;
+    const int K = num_dofs(p);
+    auto ops = std::make_shared<HostOps>();
+    std::vector<double> tmp((size_t)K * K);
+    auto put = [&](std::vector<double>& dst, int count, int kind) {
+        dst.assign((size_t)count * K * K, 0.0);
+        for (int idx = 0; idx < count; ++idx) {
+            build_operator(kind, p, idx, tmp.data());
+            double* o = dst.data() + (size_t)idx * K * K;
+            for (int j = 0; j < K; ++j)
+                for (int k = 0; k < K; ++k) o[(size_t)k * K + j] = tmp[(size_t)j * K + k];
+        }
+    };
+    put(ops->m2m, 8, 0);
+    put(ops->l2l, 8, 1);
+    put(ops->m2l, 343, 2);
+    g_ops[p] = ops;
+    return ops;
+}
+
+int ensure_operator_tables(Handle& h) {
+    if (h.ops_p == h.prm.p) return OGX_OK;
+    auto ops = host_ops(h.prm.p);
+    OGX_TRY(arena_get(h.ws, S_OPS_M2L, ops->m2l.size(), &h.d_m2l));
+    OGX_TRY(arena_get(h.ws, S_OPS_M2M, ops->m2m.size(), &h.d_m2m));
+    OGX_TRY(arena_get(h.ws, S_OPS_L2L, ops->l2l.size(), &h.d_l2l));
+    OGX_CUDA(cudaMemcpy(h.d_m2l, ops->m2l.data(), ops->m2l.size() * sizeof(double), cudaMemcpyHostToDevice));
+    OGX_CUDA(cudaMemcpy(h.d_m2m, ops->m2m.data(), ops->m2m.size() * sizeof(double), cudaMemcpyHostToDevice));
+    OGX_CUDA(cudaMemcpy(h.d_l2l, ops->l2l.data(), ops->l2l.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h.ops_p = h.prm.p;
+    return OGX_OK;
+}
+
+static std::mutex g_dev_mu;
+static std::vector<int> g_dev_ready;
+
+static int device_init(int dev) {
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    if ((int)g_dev_ready.size() <= dev) g_dev_ready.resize(dev + 1, 0);
+    if (g_dev_ready[dev]) return OGX_OK;
+    g_dev_ready[dev] = 1;
+    return OGX_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.f;
+    }
+    return ms;
+}
+
+// ---- drift / kick of VelocityVerlet3D (src3d/Integrator3D.hpp:23-40) --------------------
+__global__ void k_drift(double* pos, const double* vel, const double* acc, int64_t n3, double dt, double half_dt2) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n3) pos[i] += vel[i] * dt + acc[i] * half_dt2;
+}
+__global__ void k_kick(double* vel, const double* acc_old, const double* acc_new, int64_t n3, double half_dt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n3) vel[i] += (acc_old[i] + acc_new[i]) * half_dt;
+}
+
+static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+    h.n = n;
+    h.tree_valid = false;
+    std::memset(&h.stats, 0, sizeof(h.stats));
+    h.stats.n = n;
+    if (n == 0) return OGX_OK;
+    const cudaStream_t st = h.stream;
+    OGX_CUDA(cudaEventRecord(h.ev[0], st));
+    if (h.prm.solver == OGX_SOLVER_DIRECT) {
+        OGX_TRY(direct_eval(h, d_pos, d_mass, n, d_acc, d_pot, false));
+        OGX_CUDA(cudaEventRecord(h.ev[8], st));
+        return OGX_OK;
+    }
+    OGX_TRY(ensure_operator_tables(h));
+    OGX_TRY(tree_build(h, d_pos, d_mass, n));
+    OGX_CUDA(cudaEventRecord(h.ev[1], st));
+    OGX_TRY(lists_build(h));
+    OGX_CUDA(cudaEventRecord(h.ev[9], st));
+    h.tree_valid = true;
+    if (h.prm.precision == OGX_PREC_FP64) OGX_TRY(fmm_fp64(h, d_acc, d_pot));
+    else OGX_TRY(fmm_mixed(h, d_acc, d_pot));
+    OGX_CUDA(cudaEventRecord(h.ev[8], st));
+    const DevCounts& c = *h.h_counts;
+    h.stats.num_boxes = (int32_t)c.num_boxes;
+    h.stats.num_leaves = (int32_t)c.num_leaves;
+    h.stats.max_leaf_occupancy = c.max_leaf_occ;
+    h.stats.max_level = c.max_level;
+    h.stats.list_u = c.u_total;
+    h.stats.list_w = c.w_total;
+    h.stats.list_x = c.w_total;
+    h.stats.p2p_pairs = c.p2p_pairs;
+    h.stats.m2p_evals = c.m2p_evals;
+    h.stats.p2l_evals = c.p2l_evals;
+    h.stats.adjacency_mismatch = c.adj_mismatch;
+    return OGX_OK;
+}
+
+static void finish_stats(Handle& h) {
+    if (h.n == 0) return;
+    if (cudaEventSynchronize(h.ev[8]) != cudaSuccess) { cudaGetLastError(); return; }
+    ogx_stats& s = h.stats;
+    s.ms_total = ev_ms(h.ev[0], h.ev[8]);
+    if (h.prm.solver == OGX_SOLVER_DIRECT) return;
+    s.ms_tree = ev_ms(h.ev[0], h.ev[1]);
+    s.ms_lists = ev_ms(h.ev[1], h.ev[9]);
+    s.ms_upward = ev_ms(h.ev[2], h.ev[3]);
+    s.ms_m2l = ev_ms(h.ev[3], h.ev[4]);
+    s.ms_p2l = ev_ms(h.ev[4], h.ev[5]);
+    s.ms_downward = ev_ms(h.ev[5], h.ev[6]);
+    s.ms_leaf = ev_ms(h.ev[6], h.ev[7]);
+}
+
+}  // namespace ogx
+
+using namespace ogx;
+
+#define HANDLE(hv) Handle& h = *static_cast<Handle*>(hv)
+
+extern "C" {
+
+int ogx_params_default(ogx_params* prm) {
+    if (!prm) return OGX_ERR_INVALID;
+    std::memset(prm, 0, sizeof(*prm));
+    prm->G = 1.0;
+    prm->eps = 0.0;
+    prm->p = 8;
+    prm->leaf_capacity = 64;
+    prm->solver = OGX_SOLVER_ADAPTIVE_FMM;
+    prm->precision = OGX_PREC_FP64;
+    prm->device = 0;
+    prm->stream = nullptr;
+    return OGX_OK;
+}
+
+const char* ogx_strerror(int status) {
+    switch (status) {
+        case OGX_OK: return "ok";
+        case OGX_ERR_INVALID: return "invalid argument";
+        case OGX_ERR_CUDA: return "CUDA error";
+        case OGX_ERR_NO_DEVICE: return "no CUDA device";
+        case OGX_ERR_OOM: return "out of device memory";
+        case OGX_ERR_UNSUPPORTED: return "unsupported request";
+        case OGX_ERR_TIMEOUT: return "device wait timed out";
+        case OGX_ERR_STATE: return "call out of sequence";
+        default: return "unknown status";
+    }
+}
+
+const char* ogx_last_error_message(void) { return g_last_error.c_str(); }
+
+int ogx_create(const ogx_params* prm, void** handle) {
+    if (!prm || !handle) return OGX_ERR_INVALID;
+    *handle = nullptr;
+    if (!(std::isfinite(prm->G)) || !(prm->eps >= 0.0) || !std::isfinite(prm->eps)) return OGX_ERR_INVALID;
+    if (prm->solver != OGX_SOLVER_ADAPTIVE_FMM && prm->solver != OGX_SOLVER_DIRECT) return OGX_ERR_INVALID;
+    if (prm->precision != OGX_PREC_FP64 && prm->precision != OGX_PREC_MIXED) return OGX_ERR_INVALID;
+    if (prm->solver == OGX_SOLVER_ADAPTIVE_FMM) {
+        if (prm->p < 1 || prm->p > kPMax) return OGX_ERR_INVALID;
+        if (prm->leaf_capacity < 1 || prm->leaf_capacity > 4096) return OGX_ERR_INVALID;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_last_error(OGX_ERR_NO_DEVICE, "no CUDA device");
+        return OGX_ERR_NO_DEVICE;
+    }
+    if (prm->device < 0 || prm->device >= ndev) return OGX_ERR_INVALID;
+    DeviceGuard g(prm->device);
+    OGX_TRY(device_init(prm->device));
+    std::unique_ptr<Handle> h(new Handle);
+    h->prm = *prm;
+    h->device = prm->device;
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, prm->device);
+    if (prm->stream) {
+        h->stream = (cudaStream_t)prm->stream;
+    } else {
+        OGX_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->own_stream = true;
+    }
+    OGX_CUDA(cudaMallocHost(&h->h_counts, sizeof(DevCounts)));
+    std::memset(h->h_counts, 0, sizeof(DevCounts));
+    for (auto& e : h->ev) OGX_CUDA(cudaEventCreate(&e));
+    *handle = h.release();
+    return OGX_OK;
+}
+
+int ogx_destroy(void* handle) {
+    if (!handle) return OGX_ERR_INVALID;
+    Handle* h = static_cast<Handle*>(handle);
+    {
+        DeviceGuard g(h->device);
+        cudaStreamSynchronize(h->stream);
+        h->ws.release();
+        if (h->h_counts) cudaFreeHost(h->h_counts);
+        if (h->h_stage) cudaFreeHost(h->h_stage);
+        for (auto& e : h->ev)
+            if (e) cudaEventDestroy(e);
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+    return OGX_OK;
+}
+
+const char* ogx_name(void* handle) {
+    if (!handle) return "ogx";
+    HANDLE(handle);
+    if (h.prm.solver == OGX_SOLVER_DIRECT) return "OgxDirect3D(B200, O(N^2) FP64)";
+    return h.prm.precision == OGX_PREC_FP64 ? "OgxAdaptiveFMM3D(B200, FP64)" : "OgxAdaptiveFMM3D(B200, mixed)";
+}
+
+int ogx_eval_device(void* handle, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+    if (!handle || n < 0 || n > (int64_t)INT32_MAX / 2) return OGX_ERR_INVALID;
+    if (n > 0 && (!d_pos || !d_mass || !d_acc)) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    return eval_device(h, n, d_pos, d_mass, d_acc, d_pot);
+}
+
+int ogx_synchronize(void* handle) {
+    if (!handle) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    return OGX_OK;
+}
+
+int ogx_eval(void* handle, int64_t n, const double* pos, const double* mass, double* acc, double* pot) {
+    if (!handle || n < 0 || n > (int64_t)INT32_MAX / 2) return OGX_ERR_INVALID;
+    if (n > 0 && (!pos || !mass || !acc)) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    if (n == 0) {
+        eval_device(h, 0, nullptr, nullptr, nullptr, nullptr);
+        return OGX_OK;
+    }
+    double *dp, *dm, *da, *dpot = nullptr;
+    OGX_TRY(arena_get(h.ws, S_POS, 3 * n, &dp));
+    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
+    OGX_TRY(arena_get(h.ws, S_ACC, 3 * n, &da));
+    if (pot) OGX_TRY(arena_get(h.ws, S_POT, n, &dpot));
+    cudaEvent_t e0 = h.ev[10], e1 = h.ev[11];
+    OGX_CUDA(cudaEventRecord(e0, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(dp, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    OGX_CUDA(cudaEventRecord(e1, h.stream));
+    OGX_TRY(eval_device(h, n, dp, dm, da, dpot));
+    const float h2d = (cudaEventSynchronize(e1) == cudaSuccess) ? ev_ms(e0, e1) : 0.f;
+    OGX_CUDA(cudaEventRecord(e0, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(acc, da, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    if (pot) OGX_CUDA(cudaMemcpyAsync(pot, dpot, n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    OGX_CUDA(cudaEventRecord(e1, h.stream));
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    finish_stats(h);
+    h.stats.ms_h2d = h2d;
+    h.stats.ms_d2h = ev_ms(e0, e1);
+    return OGX_OK;
+}
+
+int ogx_last_stats(void* handle, ogx_stats* out) {
+    if (!handle || !out) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    if (h.stats.ms_total == 0.0) finish_stats(h);
+    *out = h.stats;
+    return OGX_OK;
+}
+
+// ---- device-resident leapfrog -------------------------------------------------------
+int ogx_upload(void* handle, int64_t n, const double* pos, const double* vel, const double* mass) {
+    if (!handle || n <= 0 || !pos || !vel || !mass || n > (int64_t)INT32_MAX / 2) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    double *dp, *dv, *dm, *da;
+    OGX_TRY(arena_get(h.ws, S_POS, 3 * n, &dp));
+    OGX_TRY(arena_get(h.ws, S_VEL, 3 * n, &dv));
+    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
+    OGX_TRY(arena_get(h.ws, S_ACC, 3 * n, &da));
+    OGX_CUDA(cudaMemcpyAsync(dp, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(dv, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    OGX_TRY(eval_device(h, n, dp, dm, da, nullptr));  // VelocityVerlet3D::initialize
+    h.resident = true;
+    h.n = n;
+    return OGX_OK;
+}
+
+int ogx_step(void* handle, double dt, int nsteps) {
+    if (!handle || nsteps < 0 || !std::isfinite(dt)) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    if (!h.resident) return OGX_ERR_STATE;
+    DeviceGuard g(h.device);
+    const int64_t n = h.n, n3 = 3 * n;
+    double *dp, *dv, *dm, *da, *dn;
+    OGX_TRY(arena_get(h.ws, S_POS, n3, &dp));
+    OGX_TRY(arena_get(h.ws, S_VEL, n3, &dv));
+    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
+    OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
+    OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
+    const int grid = (int)((n3 + 255) / 256);
+    for (int s = 0; s < nsteps; ++s) {
+        k_drift<<<grid, 256, 0, h.stream>>>(dp, dv, da, n3, dt, 0.5 * dt * dt);
+        OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
+        k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt);
+        OGX_CUDA(cudaMemcpyAsync(da, dn, n3 * sizeof(double), cudaMemcpyDeviceToDevice, h.stream));
+    }
+    OGX_CUDA(cudaGetLastError());
+    h.n = n;
+    return OGX_OK;
+}
+
+int ogx_download(void* handle, double* pos, double* vel, double* acc) {
+    if (!handle) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    if (!h.resident) return OGX_ERR_STATE;
+    DeviceGuard g(h.device);
+    const int64_t n3 = 3 * h.n;
+    double *dp, *dv, *da;
+    OGX_TRY(arena_get(h.ws, S_POS, n3, &dp));
+    OGX_TRY(arena_get(h.ws, S_VEL, n3, &dv));
+    OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
+    if (pos) OGX_CUDA(cudaMemcpyAsync(pos, dp, n3 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    if (vel) OGX_CUDA(cudaMemcpyAsync(vel, dv, n3 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    if (acc) OGX_CUDA(cudaMemcpyAsync(acc, da, n3 * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    return OGX_OK;
+}
+
+// ---- tree export ----------------------------------------------------------------------
+int ogx_tree_sizes(void* handle, int64_t* sizes) {
+    if (!handle || !sizes) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    if (!h.tree_valid) return OGX_ERR_STATE;
+    DeviceGuard g(h.device);
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    const TreeView& tv = h.tv;
+    std::vector<int> col((size_t)27 * tv.nb), child((size_t)8 * tv.nb), parent(tv.nb);
+    OGX_CUDA(cudaMemcpy(col.data(), tv.col, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(child.data(), tv.child, child.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(parent.data(), tv.parent, parent.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> coord((size_t)3 * tv.nb);
+    OGX_CUDA(cudaMemcpy(coord.data(), tv.coord, coord.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    int64_t ncol = 0, nv = 0;
+    for (int b = 0; b < tv.nb; ++b) {
+        for (int d = 0; d < 27; ++d) ncol += col[27 * (size_t)b + d] >= 0;
+        if (parent[b] < 0) continue;
+        const int P = parent[b];
+        const int tx = coord[3 * b] & 1, ty = coord[3 * b + 1] & 1, tz = coord[3 * b + 2] & 1;
+        for (int D = 0; D < 27; ++D) {
+            const int Q = col[27 * (size_t)P + D];
+            if (Q < 0) continue;
+            for (int s = 0; s < 8; ++s) {
+                if (child[8 * (size_t)Q + s] < 0) continue;
+                const int ox = 2 * (D % 3 - 1) + (s & 1) - tx, oy = 2 * ((D / 3) % 3 - 1) + ((s >> 1) & 1) - ty,
+                          oz = 2 * (D / 9 - 1) + ((s >> 2) & 1) - tz;
+                if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) >= 2) ++nv;
+            }
+        }
+    }
+    sizes[0] = tv.nb;
+    sizes[1] = tv.nleaf;
+    sizes[2] = ncol;
+    sizes[3] = h.h_counts->u_total;
+    sizes[4] = nv;
+    sizes[5] = h.h_counts->w_total;
+    sizes[6] = h.h_counts->w_total;
+    return OGX_OK;
+}
+
+int ogx_tree_boxes(void* handle, int32_t* boxes, double* centers, int32_t* perm) {
+    if (!handle || !boxes) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    if (!h.tree_valid) return OGX_ERR_STATE;
+    DeviceGuard g(h.device);
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    const TreeView& tv = h.tv;
+    const size_t nb = tv.nb;
+    std::vector<int> level(nb), coord(3 * nb), parent(nb), leafid(nb), pfirst(nb), pcount(nb);
+    OGX_CUDA(cudaMemcpy(level.data(), tv.level, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(coord.data(), tv.coord, 3 * nb * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(parent.data(), tv.parent, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(leafid.data(), tv.leafid, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(pfirst.data(), tv.pfirst, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(pcount.data(), tv.pcount, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t b = 0; b < nb; ++b) {
+        int32_t* r = boxes + 8 * b;
+        r[0] = level[b]; r[1] = coord[3 * b]; r[2] = coord[3 * b + 1]; r[3] = coord[3 * b + 2];
+        r[4] = parent[b]; r[5] = leafid[b] >= 0 ? 1 : 0; r[6] = pfirst[b]; r[7] = pcount[b];
+    }
+    if (centers) OGX_CUDA(cudaMemcpy(centers, tv.center, 4 * nb * sizeof(double), cudaMemcpyDeviceToHost));
+    if (perm) OGX_CUDA(cudaMemcpy(perm, tv.perm, (size_t)tv.n * sizeof(int), cudaMemcpyDeviceToHost));
+    return OGX_OK;
+}
+
+int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx) {
+    if (!handle || !off || !idx || which < 0 || which > 4) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    if (!h.tree_valid) return OGX_ERR_STATE;
+    DeviceGuard g(h.device);
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    const TreeView& tv = h.tv;
+    const size_t nb = tv.nb, nl = tv.nleaf;
+    if (which == 0 || which == 2) {
+        std::vector<int> col(27 * nb), child(8 * nb), parent(nb), coord(3 * nb);
+        OGX_CUDA(cudaMemcpy(col.data(), tv.col, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        OGX_CUDA(cudaMemcpy(child.data(), tv.child, child.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        OGX_CUDA(cudaMemcpy(parent.data(), tv.parent, nb * sizeof(int), cudaMemcpyDeviceToHost));
+        OGX_CUDA(cudaMemcpy(coord.data(), tv.coord, 3 * nb * sizeof(int), cudaMemcpyDeviceToHost));
+        int64_t e = 0;
+        for (size_t b = 0; b < nb; ++b) {
+            off[b] = e;
+            if (which == 0) {
+                for (int d = 0; d < 27; ++d)
+                    if (col[27 * b + d] >= 0) idx[e++] = col[27 * b + d];
+                continue;
+            }
+            if (parent[b] < 0) continue;
+            const int P = parent[b];
+            const int tx = coord[3 * b] & 1, ty = coord[3 * b + 1] & 1, tz = coord[3 * b + 2] & 1;
+            for (int D = 0; D < 27; ++D) {
+                const int Q = col[27 * (size_t)P + D];
+                if (Q < 0) continue;
+                for (int s = 0; s < 8; ++s) {
+                    const int c = child[8 * (size_t)Q + s];
+                    if (c < 0) continue;
+                    const int ox = 2 * (D % 3 - 1) + (s & 1) - tx, oy = 2 * ((D / 3) % 3 - 1) + ((s >> 1) & 1) - ty,
+                              oz = 2 * (D / 9 - 1) + ((s >> 2) & 1) - tz;
+                    if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) >= 2) idx[e++] = c;
+                }
+            }
+        }
+        off[nb] = e;
+        return OGX_OK;
+    }
+    if (which == 4) {
+        const int64_t nx = h.h_counts->w_total;
+        std::vector<int64_t> xo(nb + 1);
+        OGX_CUDA(cudaMemcpy(xo.data(), tv.x_off, (nb + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        std::memcpy(off, xo.data(), (nb + 1) * sizeof(int64_t));
+        if (nx) OGX_CUDA(cudaMemcpy(idx, tv.x_idx, nx * sizeof(int), cudaMemcpyDeviceToHost));
+        return OGX_OK;
+    }
+    // U (1) or W (3): per leaf CSR -> per box CSR
+    std::vector<int64_t> lo(nl + 1);
+    std::vector<int> leafbox(nl), leafid(nb);
+    const int64_t tot = (which == 1) ? h.h_counts->u_total : h.h_counts->w_total;
+    std::vector<int> li(tot > 0 ? tot : 1);
+    OGX_CUDA(cudaMemcpy(lo.data(), which == 1 ? tv.u_off : tv.w_off, (nl + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    if (tot) OGX_CUDA(cudaMemcpy(li.data(), which == 1 ? tv.u_idx : tv.w_idx, tot * sizeof(int), cudaMemcpyDeviceToHost));
+    OGX_CUDA(cudaMemcpy(leafid.data(), tv.leafid, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    int64_t e = 0;
+    for (size_t b = 0; b < nb; ++b) {
+        off[b] = e;
+        const int lf = leafid[b];
+        if (lf < 0) continue;
+        for (int64_t q = lo[lf]; q < lo[lf + 1]; ++q) idx[e++] = li[q];
+    }
+    off[nb] = e;
+    return OGX_OK;
+}
+
+}  // extern "C"
+
+namespace ogx {
+int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
+}

@@ -1,0 +1,435 @@
+// ogx_fmm64.cu -- the plain FP64 form of the adaptive FMM evaluation.
+//
+// Same passes as AdaptiveFMM3D::computeAccelerations (src3d/AdaptiveFMM3D.hpp:29-110)
+// but organised for the GPU:
+//   P2M           warp per leaf: lanes build harmonics of 32 bodies into shared
+//                 memory, then reduce columns (:53-61, FmmExpansions3D.hpp:148-163)
+//   M2M           per level bottom-up, warp per parent, level-independent
+//                 matrices MM_s (:62-71)
+//   M2L           all levels in one launch: targets grouped by their octant in
+//                 the parent, 64 per CTA; for each of the 189 (colleague slot,
+//                 child) combinations the sources of all 64 targets are gathered
+//                 into shared memory and multiplied by the offset's matrix T_o
+//                 (:78-81; V list implicit in the colleague slots)
+//   P2L           warp per box over its X list (:82, :117-128)
+//   L2L           per level top-down, warp per box (:75-77)
+//   leaf far      warp per leaf: L2P through gradient coefficients of L, M2P
+//                 over the W list through gradient coefficients of M (:92-93)
+//   leaf near     warp per leaf: softened P2P over the U list, j != i (:95-103),
+//                 then acc[orig] = G (far + near) (:104)
+// Potentials (pot = -G Phi) are produced alongside when requested.
+#include "ogx_harmonics.cuh"
+
+namespace ogx {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- P2M / P2L: particle -> expansion --------------------------------------------
+// MODE 0: P2M for leaf `lf`: coefficients q conj(R(u)), u = (x - c)/side, store.
+// MODE 1: P2L for box `b` over X(b): (q/side) conj(S(u)), accumulate.
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) k_p2x(TreeView tv, int ntargets, double* out) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int LD = K | 1;
+    extern __shared__ double s_buf[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int t = blockIdx.x * 4 + wid;
+    if (t >= ntargets) return;
+    double* buf = s_buf + (size_t)wid * 32 * LD;
+    const int b = (MODE == 0) ? tv.leafbox[t] : t;
+    int64_t e0, e1;
+    if (MODE == 0) { e0 = 0; e1 = 1; }
+    else { e0 = tv.x_off[b]; e1 = tv.x_off[b + 1]; if (e0 == e1) return; }
+    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+    const double side = 2.0 * tv.center[4 * b + 3], inv = 1.0 / side;
+    constexpr int NPL = (K + 31) / 32;
+    double acc[NPL];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) acc[q] = 0.0;
+    for (int64_t e = e0; e < e1; ++e) {
+        const int src = (MODE == 0) ? b : tv.x_idx[e];
+        const int f0 = tv.pfirst[src], cnt = tv.pcount[src];
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            const int j = j0 + lane;
+            double* row = buf + (size_t)lane * LD;
+            if (j < cnt) {
+                const int i = f0 + j;
+                const double q = tv.pm[i];
+                const double ux = (tv.px[i] - cx) * inv, uy = (tv.py[i] - cy) * inv, uz = (tv.pz[i] - cz) * inv;
+                auto put = [&](int n, int m, double re, double im) {
+                    if (m == 0) row[n * n] = q * re;
+                    else { row[n * n + 2 * m - 1] = q * re; row[n * n + 2 * m] = -q * im; }
+                };
+                if (MODE == 0) for_regular<P>(ux, uy, uz, put);
+                else for_singular<P>(ux, uy, uz, put);
+            } else {
+                for (int d = 0; d < K; ++d) row[d] = 0.0;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < NPL; ++q) {
+                const int d = lane + 32 * q;
+                if (d < K) {
+                    double s = 0.0;
+#pragma unroll 8
+                    for (int r = 0; r < 32; ++r) s += buf[(size_t)r * LD + d];
+                    acc[q] += s;
+                }
+            }
+            __syncwarp();
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) {
+        const int d = lane + 32 * q;
+        if (d < K) {
+            if (MODE == 0) out[(size_t)b * K + d] = acc[q];
+            else out[(size_t)b * K + d] += acc[q] * inv;
+        }
+    }
+}
+
+// ---- M2M (MODE 0) / L2L (MODE 1) for the boxes of one level -----------------------
+// Matrices are stored transposed (k-major) so lanes over output rows coalesce.
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) k_translate_level(TreeView tv, int first, int count, const double* opsT,
+                                                         double* mpole, double* local, const double* lown) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int NPL = (K + 31) / 32;
+    __shared__ double s_vec[4][K];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = blockIdx.x * 4 + wid;
+    if (k >= count) return;
+    const int b = first + k;
+    double acc[NPL];
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) acc[q] = 0.0;
+    if (MODE == 0) {
+        if (tv.leafid[b] >= 0) return;
+        for (int s = 0; s < 8; ++s) {
+            const int c = tv.child[8 * b + s];
+            if (c < 0) continue;
+            for (int d = lane; d < K; d += 32) s_vec[wid][d] = mpole[(size_t)c * K + d];
+            __syncwarp();
+            const double* T = opsT + (size_t)s * K * K;
+            for (int kk = 0; kk < K; ++kk) {
+                const double v = s_vec[wid][kk];
+#pragma unroll
+                for (int q = 0; q < NPL; ++q) {
+                    const int j = lane + 32 * q;
+                    if (j < K) acc[q] = fma(__ldg(T + (size_t)kk * K + j), v, acc[q]);
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int q = 0; q < NPL; ++q) {
+            const int j = lane + 32 * q;
+            if (j < K) mpole[(size_t)b * K + j] = acc[q];
+        }
+    } else {
+        const int P_ = tv.parent[b];
+        if (P_ < 0) {
+            for (int d = lane; d < K; d += 32) local[(size_t)b * K + d] = lown[(size_t)b * K + d];
+            return;
+        }
+        const int s = (tv.coord[3 * b] & 1) | ((tv.coord[3 * b + 1] & 1) << 1) | ((tv.coord[3 * b + 2] & 1) << 2);
+        for (int d = lane; d < K; d += 32) s_vec[wid][d] = local[(size_t)P_ * K + d];
+        __syncwarp();
+        const double* T = opsT + (size_t)s * K * K;
+        for (int kk = 0; kk < K; ++kk) {
+            const double v = s_vec[wid][kk];
+#pragma unroll
+            for (int q = 0; q < NPL; ++q) {
+                const int j = lane + 32 * q;
+                if (j < K) acc[q] = fma(__ldg(T + (size_t)kk * K + j), v, acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NPL; ++q) {
+            const int j = lane + 32 * q;
+            if (j < K) local[(size_t)b * K + j] = lown[(size_t)b * K + j] + acc[q];
+        }
+    }
+}
+
+// ---- M2L (structured, FP64) -----------------------------------------------------------
+constexpr int M2L_TGT = 64;
+constexpr int M2L_THREADS = 256;
+
+// One CTA = up to 64 targets that share their octant t inside the parent.
+template <int P>
+__global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uint32_t* tgt_key, const uint32_t* tgt_box,
+                                                         const double* opsT, const double* mpole, double* lown) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int LD = K | 1;
+    constexpr int NR = (K + 15) / 16;
+    extern __shared__ double s_m[];                      // [64][LD]
+    __shared__ int s_pcol[M2L_TGT][27];
+    __shared__ int s_src[M2L_TGT];
+    __shared__ int s_tgt[M2L_TGT];
+    __shared__ int s_t;
+    const int tid = threadIdx.x;
+    const int base = blockIdx.x * M2L_TGT;
+    // the padded target layout never mixes octants inside a tile
+    if (tid == 0) s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
+    __syncthreads();
+    const int t = s_t;
+    if (t < 0) return;
+    if (tid < M2L_TGT) {
+        const int i = base + tid;
+        const int b = ((int)tgt_key[i] == t) ? (int)tgt_box[i] : -1;
+        s_tgt[tid] = b;
+        const int P_ = (b >= 0) ? tv.parent[b] : -1;
+        for (int d = 0; d < 27; ++d) s_pcol[tid][d] = (P_ >= 0) ? tv.col[27 * P_ + d] : -1;
+    }
+    __syncthreads();
+    const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
+    const int tg = tid & 15, rg = tid >> 4;
+    double acc[4][NR];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int i = 0; i < NR; ++i) acc[a][i] = 0.0;
+    for (int D = 0; D < 27; ++D) {
+        const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+        for (int s = 0; s < 8; ++s) {
+            const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+            if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;  // adjacent: not in V
+            int mysrc = -1;
+            if (tid < M2L_TGT) {
+                const int Q = s_pcol[tid][D];
+                mysrc = (Q >= 0) ? tv.child[8 * Q + s] : -1;
+                s_src[tid] = mysrc;
+            }
+            if (!__syncthreads_or(mysrc >= 0)) continue;
+            for (int idx = tid; idx < M2L_TGT * K; idx += M2L_THREADS) {
+                const int r = idx / K, kk = idx - r * K;
+                const int src = s_src[r];
+                s_m[r * LD + kk] = (src >= 0) ? mpole[(size_t)src * K + kk] : 0.0;
+            }
+            __syncthreads();
+            const double* T = opsT + (size_t)((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) * K * K;
+            for (int kk = 0; kk < K; ++kk) {
+                double mv[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) mv[a] = s_m[(tg + 16 * a) * LD + kk];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const int j = rg + 16 * i;
+                    const double tv_ = (j < K) ? __ldg(T + (size_t)kk * K + j) : 0.0;
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) acc[a][i] = fma(tv_, mv[a], acc[a][i]);
+                }
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int b = s_tgt[tg + 16 * a];
+        if (b < 0) continue;
+        const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            const int j = rg + 16 * i;
+            if (j < K) lown[(size_t)b * K + j] += acc[a][i] * inv;
+        }
+    }
+}
+
+// ---- leaf far field: L2P + W-list M2P ---------------------------------------------------
+template <int P, bool POT>
+__global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const double* mpole, const double* local, double* far) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int KG = P * P;               // local gradient: degree P-1
+    constexpr int KH = (P + 2) * (P + 2);   // multipole gradient: degree P+1
+    __shared__ double s_c[4][K];
+    __shared__ double s_g[4][3][KH];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= tv.nleaf) return;
+    const int b = tv.leafbox[lf];
+    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+    const double side = 2.0 * tv.center[4 * b + 3], inv = 1.0 / side;
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int j = j0 + lane;
+        const bool act = j < cnt;
+        const int i = f0 + (act ? j : 0);
+        const double x = tv.px[i], y = tv.py[i], z = tv.pz[i];
+        double gx = 0, gy = 0, gz = 0, phi = 0;
+        // L2P
+        for (int d = lane; d < K; d += 32) s_c[wid][d] = local[(size_t)b * K + d];
+        __syncwarp();
+        for (int d = lane; d < KG; d += 32) {
+            double g[3];
+            local_grad_dof(s_c[wid], d, g);
+            s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
+        }
+        __syncwarp();
+        {
+            const double ux = (x - cx) * inv, uy = (y - cy) * inv, uz = (z - cz) * inv;
+            double ax = 0, ay = 0, az = 0, ph = 0;
+            for_regular<P>(ux, uy, uz, [&](int n, int m, double re, double im) {
+                const double w = (m == 0) ? 1.0 : 2.0;
+                const int dr = dof_re(n, m);
+                if (POT) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : 0.0));
+                if (n < P) {
+                    ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : 0.0));
+                    ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : 0.0));
+                    az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : 0.0));
+                }
+            });
+            gx = ax * inv; gy = ay * inv; gz = az * inv; phi = ph;
+        }
+        __syncwarp();
+        // M2P over W(b)
+        for (int64_t e = tv.w_off[lf]; e < tv.w_off[lf + 1]; ++e) {
+            const int c = tv.w_idx[e];
+            for (int d = lane; d < K; d += 32) s_c[wid][d] = mpole[(size_t)c * K + d];
+            __syncwarp();
+            for (int d = lane; d < KH; d += 32) {
+                double g[3];
+                mpole_grad_dof(s_c[wid], d, g);
+                s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
+            }
+            __syncwarp();
+            const double wcx = tv.center[4 * c], wcy = tv.center[4 * c + 1], wcz = tv.center[4 * c + 2];
+            const double winv = 1.0 / (2.0 * tv.center[4 * c + 3]);
+            const double ux = (x - wcx) * winv, uy = (y - wcy) * winv, uz = (z - wcz) * winv;
+            double ax = 0, ay = 0, az = 0, ph = 0;
+            for_singular<P + 1>(ux, uy, uz, [&](int n, int m, double re, double im) {
+                const double w = (m == 0) ? 1.0 : 2.0;
+                const int dr = dof_re(n, m);
+                if (POT && n <= P) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : 0.0));
+                ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : 0.0));
+                ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : 0.0));
+                az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : 0.0));
+            });
+            gx += ax * winv * winv; gy += ay * winv * winv; gz += az * winv * winv;
+            phi += ph * winv;
+            __syncwarp();
+        }
+        if (act) {
+            far[4 * (size_t)i] = gx; far[4 * (size_t)i + 1] = gy; far[4 * (size_t)i + 2] = gz; far[4 * (size_t)i + 3] = phi;
+        }
+    }
+}
+
+// ---- leaf near field (P2P over U) + final combine ----------------------------------------
+template <bool POT>
+__global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= tv.nleaf) return;
+    const int b = tv.leafbox[lf];
+    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int jj = j0 + lane;
+        const bool act = jj < cnt;
+        const int i = f0 + (act ? jj : 0);
+        const double x = tv.px[i], y = tv.py[i], z = tv.pz[i];
+        double ax = 0, ay = 0, az = 0, ph = 0;
+        for (int64_t e = tv.u_off[lf]; e < tv.u_off[lf + 1]; ++e) {
+            const int c = tv.u_idx[e];
+            const int s0 = tv.pfirst[c], sc = tv.pcount[c];
+            for (int j = s0; j < s0 + sc; ++j) {
+                const double dx = __ldg(tv.px + j) - x, dy = __ldg(tv.py + j) - y, dz = __ldg(tv.pz + j) - z;
+                const double r2 = (dx * dx + dy * dy + dz * dz) + eps2;
+                const double ir = rsqrt(r2);
+                const double mj = (j == i) ? 0.0 : __ldg(tv.pm + j);
+                const double w = mj * ir * ir * ir;
+                if (j != i) {
+                    ax = fma(w, dx, ax); ay = fma(w, dy, ay); az = fma(w, dz, az);
+                    if (POT) ph = fma(mj, ir, ph);
+                }
+            }
+        }
+        if (act) {
+            const int o = tv.perm[i];
+            acc[3 * (size_t)o] = G * (far[4 * (size_t)i] + ax);
+            acc[3 * (size_t)o + 1] = G * (far[4 * (size_t)i + 1] + ay);
+            acc[3 * (size_t)o + 2] = G * (far[4 * (size_t)i + 2] + az);
+            if (POT) pot[o] = -G * (far[4 * (size_t)i + 3] + ph);
+        }
+    }
+}
+
+// ---- dispatch --------------------------------------------------------------------------
+template <int P>
+int run_fp64(Handle& h, double* d_acc, double* d_pot) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int LD = K | 1;
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    OGX_TRY(harm_tables_ready(h.device));
+    double *M, *L, *Lown, *far;
+    OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
+    OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
+    OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
+    OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
+    OGX_CUDA(cudaEventRecord(h.ev[2], st));
+    // upward
+    const size_t p2x_smem = 4 * 32 * LD * sizeof(double);
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    k_p2x<P, 0><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M);
+    for (int l = h.max_level - 1; l >= 0; --l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr);
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[3], st));
+    // M2L
+    OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
+    if (h.ntgt > 0) {
+        const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
+        OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
+        const int ntiles = h.ntgt_pad / M2L_TGT;
+        k_m2l_fp64<P><<<ntiles, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M, Lown);
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[4], st));
+    // P2L
+    k_p2x<P, 1><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown);
+    OGX_CUDA(cudaEventRecord(h.ev[5], st));
+    // L2L top-down
+    for (int l = 0; l <= h.max_level; ++l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown);
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[6], st));
+    // leaves
+    const bool pot = d_pot != nullptr;
+    if (pot) k_leaf_far<P, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far);
+    else k_leaf_far<P, false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far);
+    const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
+    if (pot) k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot);
+    else k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr);
+    OGX_CUDA(cudaEventRecord(h.ev[7], st));
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+}  // namespace
+
+int fmm_fp64(Handle& h, double* d_acc, double* d_pot) {
+    switch (h.prm.p) {
+        case 1: return run_fp64<1>(h, d_acc, d_pot);
+        case 2: return run_fp64<2>(h, d_acc, d_pot);
+        case 3: return run_fp64<3>(h, d_acc, d_pot);
+        case 4: return run_fp64<4>(h, d_acc, d_pot);
+        case 5: return run_fp64<5>(h, d_acc, d_pot);
+        case 6: return run_fp64<6>(h, d_acc, d_pot);
+        case 7: return run_fp64<7>(h, d_acc, d_pot);
+        case 8: return run_fp64<8>(h, d_acc, d_pot);
+        case 9: return run_fp64<9>(h, d_acc, d_pot);
+        case 10: return run_fp64<10>(h, d_acc, d_pot);
+        case 11: return run_fp64<11>(h, d_acc, d_pot);
+        case 12: return run_fp64<12>(h, d_acc, d_pot);
+        default: return OGX_ERR_INVALID;
+    }
+}
+
+}  // namespace ogx

@@ -1,0 +1,201 @@
+// ogx_harmonics.cuh -- solid harmonics and expansion-coefficient helpers.
+//
+// The reference evaluates Y_n^m through cos/sin/atan2 and the seminormalised
+// Legendre recurrence (src3d/FmmExpansions3D.hpp:75-107) and multiplies by
+// rho^n or rho^-(n+1) afterwards.  Here the same functions are generated
+// directly as solid harmonics in Cartesian form, column by column in m, so a
+// thread never holds more than the current column:
+//   R_n^m = rho^n Y_n^m:           R_m^m = (x+iy) a_m R_{m-1}^{m-1}
+//                                  R_{m+1}^m = z b_m R_m^m
+//                                  R_n^m = z A_nm R_{n-1}^m - r^2 B_nm R_{n-2}^m
+//   S_n^m = Y_n^m / rho^{n+1}:     same recurrences with a factor 1/r^2 per step
+// with a_m = sqrt((2m-1)/2m), b_m = sqrt(2m+1), A_nm = (2n-1)/sqrt(n^2-m^2),
+// B_nm = sqrt((n-1)^2-m^2)/sqrt(n^2-m^2): the reference's Q recurrence
+// multiplied through by rho^n e^{i m phi} (no trigonometric calls).
+//
+// Real coefficient layout (K = (p+1)^2 doubles): dof(n,0) = n^2,
+// dof(n,m>0) = n^2 + 2m - 1 (real part), n^2 + 2m (imaginary part).
+// Negative orders follow from c_n^{-m} = conj(c_n^m) for real sources.
+#pragma once
+
+#include <cmath>
+#include <mutex>
+
+#include "ogx_internal.cuh"
+
+namespace ogx {
+
+struct HarmTables {
+    double a[kDegMax + 2];
+    double b[kDegMax + 2];
+    double A[kDegMax + 2][kDegMax + 2];
+    double B[kDegMax + 2][kDegMax + 2];
+};
+
+// One copy per translation unit (whole-program compilation, no device linking);
+// every unit that launches harmonic kernels calls harm_tables_ready() first.
+static __constant__ HarmTables c_harm;
+
+static inline int harm_tables_ready(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64) return OGX_ERR_INVALID;
+    if (done[device]) return OGX_OK;
+    HarmTables t{};
+    for (int m = 0; m < kDegMax + 2; ++m) {
+        t.a[m] = m > 0 ? std::sqrt((2.0 * m - 1.0) / (2.0 * m)) : 1.0;
+        t.b[m] = std::sqrt(2.0 * m + 1.0);
+    }
+    for (int n = 0; n < kDegMax + 2; ++n)
+        for (int m = 0; m < kDegMax + 2; ++m)
+            if (n >= m + 2) {
+                const double d = std::sqrt((double)(n * n - m * m));
+                t.A[n][m] = (2.0 * n - 1.0) / d;
+                t.B[n][m] = std::sqrt((double)((n - 1) * (n - 1) - m * m)) / d;
+            }
+    const cudaError_t e = cudaMemcpyToSymbol(c_harm, &t, sizeof(t));
+    if (e != cudaSuccess) {
+        set_last_error(OGX_ERR_CUDA, std::string("harmonic tables: ") + cudaGetErrorString(e));
+        return OGX_ERR_CUDA;
+    }
+    done[device] = true;
+    return OGX_OK;
+}
+
+__host__ __device__ __forceinline__ constexpr int dof_re(int n, int m) { return m == 0 ? n * n : n * n + 2 * m - 1; }
+
+// Visit R_n^m(x,y,z), n <= P (m >= 0), calling f(n, m, re, im) column by column.
+template <int P, class T, class F>
+__device__ __forceinline__ void for_regular(T x, T y, T z, F&& f) {
+    const T r2 = x * x + y * y + z * z;
+    T dr = 1, di = 0;  // R_m^m
+#pragma unroll
+    for (int m = 0; m <= P; ++m) {
+        if (m > 0) {
+            const T a = (T)c_harm.a[m];
+            const T nr = a * (x * dr - y * di), ni = a * (x * di + y * dr);
+            dr = nr;
+            di = ni;
+        }
+        f(m, m, dr, di);
+        if (m + 1 <= P) {
+            const T bz = (T)c_harm.b[m] * z;
+            T pr = dr, pi = di;              // R_{n-2}
+            T cr = bz * dr, ci = bz * di;    // R_{n-1}
+            f(m + 1, m, cr, ci);
+#pragma unroll
+            for (int n = m + 2; n <= P; ++n) {
+                const T A = (T)c_harm.A[n][m] * z, B = (T)c_harm.B[n][m] * r2;
+                const T qr = A * cr - B * pr, qi = A * ci - B * pi;
+                pr = cr; pi = ci; cr = qr; ci = qi;
+                f(n, m, cr, ci);
+            }
+        }
+    }
+}
+
+// Visit S_n^m(x,y,z), n <= P (m >= 0).  The origin is excluded by construction
+// (sources and targets of M2P/P2L are in well-separated boxes).
+template <int P, class T, class F>
+__device__ __forceinline__ void for_singular(T x, T y, T z, F&& f) {
+    const T r2 = x * x + y * y + z * z;
+    const T ir2 = T(1) / r2;
+    T dr = sqrt(ir2), di = 0;  // S_0^0 = 1/rho
+#pragma unroll
+    for (int m = 0; m <= P; ++m) {
+        if (m > 0) {
+            const T a = (T)c_harm.a[m] * ir2;
+            const T nr = a * (x * dr - y * di), ni = a * (x * di + y * dr);
+            dr = nr;
+            di = ni;
+        }
+        f(m, m, dr, di);
+        if (m + 1 <= P) {
+            const T bz = (T)c_harm.b[m] * z * ir2;
+            T pr = dr, pi = di;
+            T cr = bz * dr, ci = bz * di;
+            f(m + 1, m, cr, ci);
+#pragma unroll
+            for (int n = m + 2; n <= P; ++n) {
+                const T A = (T)c_harm.A[n][m] * z * ir2, B = (T)c_harm.B[n][m] * ir2;
+                const T qr = A * cr - B * pr, qi = A * ci - B * pi;
+                pr = cr; pi = ci; cr = qr; ci = qi;
+                f(n, m, cr, ci);
+            }
+        }
+    }
+}
+
+// complex coefficient c_n^m from a real layout (m may be negative)
+template <class T>
+__device__ __forceinline__ void coef_get(const T* c, int n, int m, T& re, T& im) {
+    if (m < -n || m > n || n < 0) { re = 0; im = 0; return; }
+    if (m == 0) { re = c[n * n]; im = 0; return; }
+    const int am = m < 0 ? -m : m;
+    re = c[n * n + 2 * am - 1];
+    im = c[n * n + 2 * am];
+    if (m < 0) im = -im;
+}
+
+// Gradient coefficients of a local expansion (degree P -> P-1), in the real
+// layout, for the three axes.  From the derivative recurrences of
+// FmmExpansions3D.hpp:111-119 as used by localField (:215-235):
+//   Gz_n^m = cz_R(n+1,m) L_{n+1}^m
+//   Gx_n^m = (cp_R(n+1,m-1) L_{n+1}^{m-1} + cm_R(n+1,m+1) L_{n+1}^{m+1}) / 2
+//   Gy_n^m = -i (cp_R(n+1,m-1) L_{n+1}^{m-1} - cm_R(n+1,m+1) L_{n+1}^{m+1}) / 2
+// Every returned value is for one real dof index `d` of degree <= P-1.
+template <class T>
+__device__ __forceinline__ void local_grad_dof(const T* L, int d, T g[3]) {
+    const int n = (int)floorf(sqrtf((float)d) + 1e-4f);
+    const int r = d - n * n;
+    const int m = (r + 1) >> 1;
+    const int part = (r == 0) ? 0 : ((r - 1) & 1);
+    const int N = n + 1;
+    T lr, li, pr, pi, mr, mi;
+    coef_get(L, N, m, lr, li);
+    coef_get(L, N, m - 1, mr, mi);   // L_{n+1}^{m-1}
+    coef_get(L, N, m + 1, pr, pi);   // L_{n+1}^{m+1}
+    const T czr = sqrt((T)(N * N - m * m));
+    const int mm = m - 1, mp = m + 1;
+    const T cpr = ((mm >= 0) ? -1 : 1) * sqrt((T)((N - mm) * (N - mm - 1)));
+    const T cmr = ((mp > 0) ? 1 : -1) * sqrt((T)((N + mp) * (N + mp - 1)));
+    const T xr = T(0.5) * (cpr * mr + cmr * pr), xi = T(0.5) * (cpr * mi + cmr * pi);
+    // -i/2 (a - b) = (Im(a-b)/2) - i (Re(a-b)/2)
+    const T dr = cpr * mr - cmr * pr, di = cpr * mi - cmr * pi;
+    const T yr = T(0.5) * di, yi = T(-0.5) * dr;
+    const T zr = czr * lr, zi = czr * li;
+    if (part == 0) { g[0] = xr; g[1] = yr; g[2] = zr; }
+    else { g[0] = xi; g[1] = yi; g[2] = zi; }
+}
+
+// Gradient coefficients of a multipole expansion (degree P -> P+1), from
+// dz_S/dp_S/dm_S (FmmExpansions3D.hpp:121-129) as used by multipoleField (:180-200):
+//   Hz_n^m = dz_S(n-1,m) M_{n-1}^m
+//   Hx_n^m = (dp_S(n-1,m-1) M_{n-1}^{m-1} + dm_S(n-1,m+1) M_{n-1}^{m+1}) / 2
+//   Hy_n^m = -i (dp_S(n-1,m-1) M_{n-1}^{m-1} - dm_S(n-1,m+1) M_{n-1}^{m+1}) / 2
+template <class T>
+__device__ __forceinline__ void mpole_grad_dof(const T* M, int d, T g[3]) {
+    const int n = (int)floorf(sqrtf((float)d) + 1e-4f);
+    const int r = d - n * n;
+    const int m = (r + 1) >> 1;
+    const int part = (r == 0) ? 0 : ((r - 1) & 1);
+    if (n == 0) { g[0] = g[1] = g[2] = 0; return; }
+    const int N = n - 1;
+    T lr, li, pr, pi, mr, mi;
+    coef_get(M, N, m, lr, li);
+    coef_get(M, N, m - 1, mr, mi);
+    coef_get(M, N, m + 1, pr, pi);
+    const T dzs = -sqrt((T)((N + 1) * (N + 1) - m * m));
+    const int mm = m - 1, mp = m + 1;
+    const T dps = ((mm >= 0) ? -1 : 1) * sqrt((T)((N + mm + 1) * (N + mm + 2)));
+    const T dms = ((mp > 0) ? 1 : -1) * sqrt((T)((N - mp + 1) * (N - mp + 2)));
+    const T xr = T(0.5) * (dps * mr + dms * pr), xi = T(0.5) * (dps * mi + dms * pi);
+    const T dr = dps * mr - dms * pr, di = dps * mi - dms * pi;
+    const T yr = T(0.5) * di, yi = T(-0.5) * dr;
+    const T zr = (m <= N) ? dzs * lr : T(0), zi = (m <= N) ? dzs * li : T(0);
+    if (part == 0) { g[0] = xr; g[1] = yr; g[2] = zr; }
+    else { g[0] = xi; g[1] = yi; g[2] = zi; }
+}
+
+}  // namespace ogx

@@ -1,0 +1,200 @@
+// ogx_internal.cuh -- shared declarations of the B200 adaptive-FMM library.
+//
+// Data layout in HBM (one handle, one system):
+//   bodies   : original order pos (n x 3 f64, caller's Vec3 AoS), mass (n f64)
+//              sorted order px/py/pz/m (SoA f64), perm (sorted -> original)
+//   keys     : 72-bit octant path (24 levels x 3 bits) as (hi u64: levels 1..21,
+//              lo u32: levels 22..24), the exact octant tests of
+//              AdaptiveOctree::subdivide (src3d/AdaptiveOctree.hpp:109-127)
+//   boxes    : level-major, Morton order within a level; per box level, int
+//              coords, FP64 centre/half (same arithmetic as the reference),
+//              parent, child[8], leaf id, pfirst/pcount, colleague[27] by
+//              relative offset slot (dx+1)+3(dy+1)+9(dz+1)
+//   lists    : U, W per leaf and X per box as CSR; V is implicit in the
+//              colleague slots (children of the parent's colleagues)
+//   expansions: scaled real coefficients, K = (p+1)^2 doubles per box:
+//              dof(n,0)=n^2, dof(n,m>0)=n^2+2m-1 (re), n^2+2m (im);
+//              M'_n = M_n / side^n, L'_n = L_n * side^n, so every translation
+//              operator is a level-independent K x K matrix.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/ogx.h"
+
+namespace ogx {
+
+constexpr int kMaxDepth = 24;     // AdaptiveOctree::maxDepth (src3d/AdaptiveOctree.hpp:49)
+constexpr int kHiLevels = 21;     // levels packed in the 64-bit key word
+constexpr int kPMax = 12;         // largest supported expansion order
+constexpr int kDegMax = kPMax + 2;
+
+inline int num_dofs(int p) { return (p + 1) * (p + 1); }
+
+// ---- error plumbing ------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define OGX_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e__ = (call);                                                        \
+        if (e__ != cudaSuccess) {                                                        \
+            ::ogx::set_last_error(OGX_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+            return (e__ == cudaErrorMemoryAllocation) ? OGX_ERR_OOM : OGX_ERR_CUDA;      \
+        }                                                                                \
+    } while (0)
+
+#define OGX_TRY(expr)                \
+    do {                             \
+        int s__ = (expr);            \
+        if (s__ != OGX_OK) return s__; \
+    } while (0)
+
+void set_last_error(int code, const std::string& msg);
+
+// ---- device buffer arena: grow-only named slots -----------------------------
+enum Slot {
+    S_POS, S_MASS, S_ACC, S_POT, S_VEL, S_ACC_OLD,
+    S_BBOX, S_ROOT, S_KHI, S_KLO, S_IDX, S_KHI2, S_KLO2, S_IDX2,
+    S_RS_HIST, S_TOPO_D, S_TOPO_CPL, S_TOPO_L, S_TOPO_CNT, S_TOPO_COFF, S_TOPO_LEAFSCAN,
+    S_LEAFSTART, S_REC_KEY, S_REC_POS, S_REC_KEY2, S_REC_POS2, S_COUNTS,
+    S_LEAFKEY, S_LEAFKEY2, S_PERM, S_PERM2,
+    S_PX, S_PY, S_PZ, S_PM,
+    S_BOX_LEVEL, S_BOX_POS, S_BOX_COORD, S_BOX_CENTER, S_BOX_PARENT, S_BOX_CHILD, S_BOX_LEAFID,
+    S_BOX_PFIRST, S_BOX_PCOUNT, S_BOX_COL, S_LEAF_BOX,
+    S_U_CNT, S_W_CNT, S_U_OFF, S_W_OFF, S_U_IDX, S_W_IDX,
+    S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, S_X_OFF, S_X_IDX, S_X_CNT, S_PERM_FINAL,
+    S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, S_TGT_TILE, S_TGT_PKEY, S_TGT_PBOX,
+    S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
+    S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
+    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN,
+    S_NUM_SLOTS
+};
+
+struct Arena {
+    void* ptr[S_NUM_SLOTS] = {};
+    size_t cap[S_NUM_SLOTS] = {};
+    size_t total = 0;
+    int get(Slot s, size_t bytes, void** out);
+    void release();
+};
+
+template <class T>
+inline int arena_get(Arena& a, Slot s, size_t count, T** out) {
+    void* p = nullptr;
+    int rc = a.get(s, count * sizeof(T) + 16, &p);
+    *out = (T*)p;
+    return rc;
+}
+
+// ---- root box of the octree (AdaptiveOctree::build, src3d/AdaptiveOctree.hpp:71-81)
+struct RootInfo {
+    double c[3];
+    double half;
+    double tol;
+    int leps;   // first level whose box edge 2*half <= eps floor (kMaxDepth+1 if none)
+    int pad;
+};
+
+// counts produced on the device and read back at the two host sync points
+struct DevCounts {
+    int64_t num_boxes;
+    int64_t num_leaves;
+    int32_t level_hist[kMaxDepth + 2];  // boxes per level (difference form before finalise)
+    int32_t max_level;
+    int32_t max_leaf_occ;
+    int64_t u_total, w_total;
+    int64_t p2p_pairs, m2p_evals, p2l_evals;
+    int64_t adj_mismatch;
+    int32_t nonleaf_level[kMaxDepth + 2];
+};
+
+// device view of the tree handed to kernels
+struct TreeView {
+    int n, nb, nleaf;
+    const RootInfo* root;
+    const double *px, *py, *pz, *pm;   // sorted bodies
+    const int* perm;                   // sorted -> original
+    const int* level;                  // per box
+    const int* coord;                  // per box: ix, iy, iz (3 ints)
+    const double* center;              // per box: cx, cy, cz, half
+    const int* parent;
+    const int* child;                  // 8 per box
+    const int* leafid;                 // per box, -1 if not leaf
+    const int* pfirst;
+    const int* pcount;
+    const int* col;                    // 27 per box
+    const int* leafbox;                // per leaf
+    const int64_t *u_off, *w_off;      // per leaf (nleaf+1)
+    const int *u_idx, *w_idx;
+    const int64_t* x_off;              // per box (nb+1)
+    const int* x_idx;
+};
+
+struct Handle {
+    ogx_params prm{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int num_sms = 148;
+    Arena ws;
+    DevCounts* h_counts = nullptr;  // pinned
+    int64_t n_cap_host = 0;
+    double* h_stage = nullptr;      // pinned staging for host-buffer calls
+    size_t h_stage_cap = 0;
+    ogx_stats stats{};
+    std::vector<int32_t> level_off;  // host copy of level offsets (num levels + 1)
+    int max_level = 0;
+    int64_t n = 0;
+    // operator tables for prm.p (host built, device resident)
+    int ops_p = -1;
+    double* d_m2l = nullptr;  // 343 x K x K
+    double* d_m2m = nullptr;  // 8 x K x K
+    double* d_l2l = nullptr;  // 8 x K x K
+    // device-resident integrator state
+    bool resident = false;
+    cudaEvent_t ev[12] = {};
+    TreeView tv{};
+    bool tree_valid = false;
+    // mixed-precision tables
+    float* d_m2l_tf32 = nullptr;
+    int mix_ready_p = -1;
+    // M2L targets (levels >= 2) sorted by child octant
+    int ntgt = 0;
+    const uint32_t* tgt_key = nullptr;
+    const uint32_t* tgt_box = nullptr;
+    int ntgt_pad = 0;                     // padded per-octant layout, 64 per tile
+    const uint32_t* tgt_tile_key = nullptr;
+    const uint32_t* tgt_tile_box = nullptr;
+};
+
+// ---- host-side operator tables (ogx_tables.cpp) -----------------------------
+// kind 0: M2M for child octant index (0..7), maps child M' -> parent M'
+// kind 1: L2L for child octant index (0..7), maps parent L' -> child L'
+// kind 2: M2L for offset index (ox+3)+7(oy+3)+49(oz+3), source minus target in
+//         units of the box side; maps source M' -> target L' * side
+void build_operator(int kind, int p, int index, double* out /* K*K row-major */);
+
+// ---- phases (defined in the .cu files) -------------------------------------
+int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);
+int lists_build(Handle& h);
+int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
+int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
+int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
+                double* d_pot, bool fp32);
+int ensure_operator_tables(Handle& h);
+
+// generic radix sort helpers (ogx_sort.cu)
+int radix_sort_u32(Handle& h, Slot kin, Slot vin, Slot kalt, Slot valt, int64_t n, int bits,
+                   uint32_t** kout, uint32_t** vout);
+int radix_sort_key72(Handle& h, int64_t n, uint64_t** khi, uint32_t** klo, uint32_t** idx);
+int scan_i32_to_i64(Handle& h, const int* in, int64_t* out, int64_t n);  // exclusive, out[n] = total
+
+}  // namespace ogx

@@ -1,0 +1,669 @@
+// ogx_tree.cu -- adaptive octree and CGR interaction lists on the GPU.
+//
+// Replaces AdaptiveOctree::build/subdivide/buildLists
+// (src3d/AdaptiveOctree.hpp:65-189), which the reference runs recursively on
+// one CPU core.  The boxes, body order and U/V/W/X lists produced here are
+// the reference's as sets (box numbering differs: level-major, Morton order
+// within a level).
+//
+// Tree, without recursion:
+//  1. root cube from a min/max reduction, same FP64 arithmetic as :71-81;
+//  2. per body the 24-level octant path, replaying the reference's FP64
+//     comparisons against the recursively shifted centres (:109-127), packed
+//     as a 72-bit key; stable radix sort by key;
+//  3. a box at level l with count > thr splits (with the eps floor and depth
+//     cap of :102-103).  Count > thr at level l for the box holding sorted
+//     position i  <=>  some window [j, j+thr] containing i has common key
+//     prefix >= l.  A sliding-window max of cpl(j, j+thr) gives every body's
+//     leaf level in O(n) with no level-by-level recursion;
+//  4. box records (level, first position) are emitted per position and
+//     stably sorted by level -> level-major box ids; parents by binary search;
+//  5. bodies are stably re-sorted by leaf id from the original order, which
+//     reproduces the reference's within-leaf order (original index order).
+// Lists:
+//  - colleagues: level-synchronous from the parent's colleagues' children,
+//    stored in 27 offset slots (:143-151);
+//  - V is implicit: children of the parent's colleagues at integer offset
+//    max|o| >= 2 (:154-161); the FP64 adjacency predicate is re-evaluated on
+//    every candidate and disagreements are counted (expected 0);
+//  - U/W per leaf (:164-169,176-189): same-level and coarser adjacent leaves
+//    come from the colleague slots of the leaf and its ancestors, finer ones
+//    from a bounded explicit-stack descent of non-leaf colleagues;
+//  - X = transpose of W via a stable sort (:171-173).
+#include "ogx_internal.cuh"
+
+namespace ogx {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- 1. root cube -----------------------------------------------------------
+__global__ void k_bbox_partial(const double* pos, int64_t n, double* part) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double v = pos[3 * i + a];
+            lo[a] = fmin(lo[a], v);
+            hi[a] = fmax(hi[a], v);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fmin(lo[a], __shfl_xor_sync(FULL, lo[a], o));
+            hi[a] = fmax(hi[a], __shfl_xor_sync(FULL, hi[a], o));
+        }
+    __shared__ double sh[32][6];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) { sh[w][a] = lo[a]; sh[w][3 + a] = hi[a]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww)
+            for (int a = 0; a < 3; ++a) { sh[0][a] = fmin(sh[0][a], sh[ww][a]); sh[0][3 + a] = fmax(sh[0][3 + a], sh[ww][3 + a]); }
+        for (int a = 0; a < 6; ++a) part[6 * blockIdx.x + a] = sh[0][a];
+    }
+}
+
+// AdaptiveOctree::build :71-81; eps-floor level from subdivide :102
+__global__ void k_bbox_final(const double* part, int nparts, double eps_floor, RootInfo* root) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int b = 0; b < nparts; ++b)
+        for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], part[6 * b + a]); hi[a] = fmax(hi[a], part[6 * b + 3 + a]); }
+    RootInfo r;
+    for (int a = 0; a < 3; ++a) r.c[a] = __dmul_rn(0.5, __dadd_rn(lo[a], hi[a]));
+    double ext = __dsub_rn(hi[0], lo[0]);
+    const double e1 = __dsub_rn(hi[1], lo[1]), e2 = __dsub_rn(hi[2], lo[2]);
+    if (ext < e1) ext = e1;
+    if (ext < e2) ext = e2;
+    double half = __dmul_rn(0.5, ext);
+    if (!(half > 0)) half = 1.0;
+    half = __dmul_rn(half, 1.0 + 1e-9);
+    r.half = half;
+    r.tol = __dmul_rn(1e-9, half);
+    int leps = kMaxDepth + 1;
+    double h = half;
+    for (int l = 0; l <= kMaxDepth; ++l) {
+        if (__dmul_rn(2.0, h) <= eps_floor) { leps = l; break; }
+        h = __dmul_rn(0.5, h);
+    }
+    r.leps = leps;
+    r.pad = 0;
+    *root = r;
+}
+
+// ---- 2. octant keys -----------------------------------------------------------
+__global__ void k_keys(const double* pos, int64_t n, const RootInfo* root, uint64_t* khi, uint32_t* klo, uint32_t* idx) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    double cx = root->c[0], cy = root->c[1], cz = root->c[2], h = root->half;
+    uint64_t hi = 0;
+    uint32_t lo = 0;
+#pragma unroll 1
+    for (int l = 1; l <= kMaxDepth; ++l) {
+        const int bx = x >= cx, by = y >= cy, bz = z >= cz;
+        const uint32_t o = (uint32_t)(bx | (by << 1) | (bz << 2));
+        const double h2 = __dmul_rn(0.5, h);
+        cx = __dadd_rn(cx, bx ? h2 : -h2);
+        cy = __dadd_rn(cy, by ? h2 : -h2);
+        cz = __dadd_rn(cz, bz ? h2 : -h2);
+        h = h2;
+        if (l <= kHiLevels) hi = (hi << 3) | o;
+        else lo = (lo << 3) | o;
+    }
+    khi[i] = hi;
+    klo[i] = lo;
+    idx[i] = (uint32_t)i;
+}
+
+__device__ __forceinline__ int cpl72(uint64_t ha, uint32_t la, uint64_t hb, uint32_t lb) {
+    const uint64_t x = ha ^ hb;
+    if (x) return (__clzll((long long)x) - 1) / 3;
+    const uint32_t y = la ^ lb;
+    if (y) return kHiLevels + (__clz((int)y) - 23) / 3;
+    return kMaxDepth;
+}
+__device__ __forceinline__ int key_digit(uint64_t hi, uint32_t lo, int level) {
+    return level <= kHiLevels ? (int)((hi >> (3 * (kHiLevels - level))) & 7ull) : (int)((lo >> (3 * (kMaxDepth - level))) & 7u);
+}
+
+// ---- 3. topology per sorted position ------------------------------------------
+__global__ void k_topo_pairs(const uint64_t* khi, const uint32_t* klo, int64_t n, int thr, int* dfirst, signed char* cplthr) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t hi = khi[i];
+    const uint32_t lo = klo[i];
+    dfirst[i] = (i == 0) ? 0 : cpl72(khi[i - 1], klo[i - 1], hi, lo) + 1;
+    cplthr[i] = (i + thr < n) ? (signed char)cpl72(hi, lo, khi[i + thr], klo[i + thr]) : (signed char)-1;
+}
+
+constexpr int WM_BLOCK = 1024;
+// leaf level L(i) = min(W(i)+1, leps, maxDepth), W = window max of cplthr over [i-thr, i].
+// Also box-start count c_i, leaf-start flag, level histogram (difference form).
+__global__ void __launch_bounds__(WM_BLOCK) k_topo_levels(const signed char* cplthr, const int* dfirst, int64_t n, int thr,
+                                                          const RootInfo* root, int* leaflev, int* cnt, int* leafflag,
+                                                          DevCounts* counts) {
+    extern __shared__ signed char s_cpl[];
+    __shared__ int s_hist[kMaxDepth + 2];
+    const int64_t b0 = (int64_t)blockIdx.x * WM_BLOCK;
+    const int win = thr + 1;
+    const int span = WM_BLOCK + win - 1;
+    for (int k = threadIdx.x; k < span; k += WM_BLOCK) {
+        const int64_t j = b0 - (win - 1) + k;
+        s_cpl[k] = (j >= 0 && j < n) ? cplthr[j] : (signed char)-1;
+    }
+    if (threadIdx.x < kMaxDepth + 2) s_hist[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = b0 + threadIdx.x;
+    if (i < n) {
+        int w = -1;
+        for (int k = 0; k < win; ++k) w = max(w, (int)s_cpl[threadIdx.x + k]);
+        int L = w + 1;
+        L = min(L, root->leps);
+        L = min(L, kMaxDepth);
+        const int d = dfirst[i];
+        const int from = (i == 0) ? 0 : d;
+        const int c = max(0, L - from + 1);
+        leaflev[i] = L;
+        cnt[i] = c;
+        leafflag[i] = (i == 0 || d <= L) ? 1 : 0;
+        if (c > 0) {
+            atomicAdd(&s_hist[from], 1);
+            atomicAdd(&s_hist[L + 1], -1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kMaxDepth + 2 && s_hist[threadIdx.x] != 0) atomicAdd(&counts->level_hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+__global__ void k_counts_finalize(DevCounts* counts, const int64_t* recoff, const int64_t* leafscan, int64_t n, int* level_off_dev) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    counts->num_boxes = recoff[n];
+    counts->num_leaves = leafscan[n];
+    int run = 0, maxl = 0;
+    int cum = 0;
+    level_off_dev[0] = 0;
+    for (int l = 0; l <= kMaxDepth; ++l) {
+        run += counts->level_hist[l];   // boxes at level l
+        counts->level_hist[l] = run;
+        if (run > 0) maxl = l;
+        cum += run;
+        level_off_dev[l + 1] = cum;
+    }
+    counts->level_hist[kMaxDepth + 1] = 0;
+    counts->max_level = maxl;
+}
+
+__global__ void k_emit_records(const int* cnt, const int* dfirst, const int* leaflev, const int64_t* recoff, int64_t n,
+                               uint32_t* reckey, uint32_t* recpos, const int* leafflag, const int64_t* leafscan,
+                               int* leafstart) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) { leafstart[leafscan[n]] = (int)n; return; }
+    const int c = cnt[i];
+    if (c > 0) {
+        const int from = (i == 0) ? 0 : dfirst[i];
+        const int64_t o = recoff[i];
+        for (int k = 0; k < c; ++k) {
+            reckey[o + k] = (uint32_t)(from + k);
+            recpos[o + k] = (uint32_t)i;
+        }
+    }
+    if (leafflag[i]) leafstart[leafscan[i]] = (int)i;
+}
+
+// ---- 4. boxes -------------------------------------------------------------------
+__global__ void k_boxes(int nb, const uint32_t* reclev, const uint32_t* recpos, const int* level_off, const uint64_t* khi,
+                        const uint32_t* klo, const int* leaflev, const int64_t* leafscan, const int* leafstart,
+                        const RootInfo* root, int* level, int* coord, double* center, int* parent, int* child, int* leafid,
+                        int* pfirst, int* pcount, int* leafbox) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb) return;
+    const int l = (int)reclev[k];
+    const int s = (int)recpos[k];
+    const uint64_t hi = khi[s];
+    const uint32_t lo = klo[s];
+    double cx = root->c[0], cy = root->c[1], cz = root->c[2], h = root->half;
+    int ix = 0, iy = 0, iz = 0;
+    for (int lv = 1; lv <= l; ++lv) {
+        const int o = key_digit(hi, lo, lv);
+        const int bx = o & 1, by = (o >> 1) & 1, bz = (o >> 2) & 1;
+        const double h2 = __dmul_rn(0.5, h);
+        cx = __dadd_rn(cx, bx ? h2 : -h2);
+        cy = __dadd_rn(cy, by ? h2 : -h2);
+        cz = __dadd_rn(cz, bz ? h2 : -h2);
+        h = h2;
+        ix = 2 * ix + bx;
+        iy = 2 * iy + by;
+        iz = 2 * iz + bz;
+    }
+    level[k] = l;
+    coord[3 * k] = ix; coord[3 * k + 1] = iy; coord[3 * k + 2] = iz;
+    center[4 * k] = cx; center[4 * k + 1] = cy; center[4 * k + 2] = cz; center[4 * k + 3] = h;
+    pfirst[k] = s;
+    const bool isleaf = leaflev[s] == l;
+    if (isleaf) {
+        const int lf = (int)leafscan[s];
+        leafid[k] = lf;
+        leafbox[lf] = k;
+        pcount[k] = leafstart[lf + 1] - s;
+    } else {
+        leafid[k] = -1;
+    }
+    if (l == 0) { parent[k] = -1; return; }
+    // parent: last box of level l-1 whose first position <= s
+    int lo_i = level_off[l - 1], hi_i = level_off[l] - 1;
+    while (lo_i < hi_i) {
+        const int mid = (lo_i + hi_i + 1) >> 1;
+        if ((int)recpos[mid] <= s) lo_i = mid; else hi_i = mid - 1;
+    }
+    parent[k] = lo_i;
+    child[8 * lo_i + key_digit(hi, lo, l)] = k;
+}
+
+__global__ void k_pcount_up(int nleaf, const int* leafbox, const int* parent, int* pcount, DevCounts* counts) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= nleaf) return;
+    const int b = leafbox[lf];
+    const int c = pcount[b];
+    atomicMax(&counts->max_leaf_occ, c);
+    for (int a = parent[b]; a >= 0; a = parent[a]) atomicAdd(&pcount[a], c);
+}
+
+// ---- 5. final body order ----------------------------------------------------------
+__global__ void k_leafkey(const uint32_t* perm_key, const int64_t* leafscan, int64_t n, uint32_t* leafkey, uint32_t* ident) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    leafkey[perm_key[i]] = (uint32_t)(leafscan[i + 1] - 1);  // leaf id containing sorted position i
+    ident[i] = (uint32_t)i;
+}
+__global__ void k_gather_bodies(const uint32_t* perm, const double* pos, const double* mass, int64_t n, int* perm_out,
+                                double* px, double* py, double* pz, double* pm) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t j = perm[i];
+    perm_out[i] = (int)j;
+    px[i] = pos[3 * j]; py[i] = pos[3 * j + 1]; pz[i] = pos[3 * j + 2];
+    pm[i] = mass[j];
+}
+
+// ---- lists ------------------------------------------------------------------------
+__device__ __forceinline__ bool adjacent64(const double* ctr, int a, int b, double tol) {
+    // AdaptiveOctree::adjacent (src3d/AdaptiveOctree.hpp:58-62)
+    const double s = __dadd_rn(__dadd_rn(ctr[4 * a + 3], ctr[4 * b + 3]), tol);
+    return fabs(__dsub_rn(ctr[4 * a], ctr[4 * b])) <= s && fabs(__dsub_rn(ctr[4 * a + 1], ctr[4 * b + 1])) <= s &&
+           fabs(__dsub_rn(ctr[4 * a + 2], ctr[4 * b + 2])) <= s;
+}
+
+__global__ void k_root_col(int* col) {
+    const int d = threadIdx.x;
+    if (d < 27) col[d] = (d == 13) ? 0 : -1;
+}
+
+// colleagues of the boxes of one level, from the parent's colleague slots
+__global__ void k_colleagues(int first, int count, const int* parent, const int* coord, const int* child, const double* ctr,
+                             const RootInfo* root, int* col, DevCounts* counts) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int b = first + k;
+    const int P = parent[b];
+    const int tx = coord[3 * b] & 1, ty = coord[3 * b + 1] & 1, tz = coord[3 * b + 2] & 1;
+    int mine[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d) mine[d] = -1;
+    const double tol = root->tol;
+    int mism = 0;
+    for (int D = 0; D < 27; ++D) {
+        const int Q = col[27 * P + D];
+        if (Q < 0) continue;
+        const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+        for (int s = 0; s < 8; ++s) {
+            const int c = child[8 * Q + s];
+            if (c < 0) continue;
+            const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+            const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
+            if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
+            if (adj_i) mine[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] = c;
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 27; ++d) col[27 * b + d] = mine[d];
+    if (mism) atomicAdd((unsigned long long*)&counts->adj_mismatch, (unsigned long long)mism);
+}
+
+constexpr int UW_STACK = 256;
+
+// U and W of one leaf (AdaptiveOctree::buildLists :164-169 with collectAdjLeaves
+// :176-180 and descendW :181-189).  FILL=false counts, FILL=true writes.
+template <bool FILL>
+__global__ void k_uw(int nleaf, const int* leafbox, const int* parent, const int* child, const int* leafid, const int* col,
+                     const double* ctr, const int* pcount, const RootInfo* root, int* ucnt, int* wcnt, const int64_t* uoff,
+                     const int64_t* woff, int* uidx, int* widx, DevCounts* counts) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= nleaf) return;
+    const int b = leafbox[lf];
+    const double tol = root->tol;
+    int64_t nu = 0, nw = 0;
+    int64_t ub = FILL ? uoff[lf] : 0, wb = FILL ? woff[lf] : 0;
+    int64_t upairs = 0;
+    auto addU = [&](int c) {
+        if (FILL) uidx[ub + nu] = c;
+        ++nu;
+        if (!FILL) upairs += pcount[c];
+    };
+    // same level (includes b itself)
+    for (int d = 0; d < 27; ++d) {
+        const int c = col[27 * b + d];
+        if (c >= 0 && leafid[c] >= 0) addU(c);
+    }
+    // coarser adjacent leaves: colleagues of ancestors
+    for (int A = parent[b]; A >= 0; A = parent[A])
+        for (int d = 0; d < 27; ++d) {
+            const int c = col[27 * A + d];
+            if (c >= 0 && leafid[c] >= 0 && adjacent64(ctr, c, b, tol)) addU(c);
+        }
+    // finer: descend non-leaf colleagues
+    int stk[UW_STACK];
+    int sp = 0;
+    bool overflow = false;
+    for (int d = 0; d < 27; ++d) {
+        const int c = col[27 * b + d];
+        if (c < 0 || c == b || leafid[c] >= 0) continue;
+        stk[sp++] = c;
+        while (sp > 0) {
+            const int node = stk[--sp];
+            for (int s = 0; s < 8; ++s) {
+                const int ch = child[8 * node + s];
+                if (ch < 0) continue;
+                if (!adjacent64(ctr, ch, b, tol)) {
+                    if (FILL) widx[wb + nw] = ch;
+                    ++nw;
+                } else if (leafid[ch] >= 0) {
+                    addU(ch);
+                } else if (sp < UW_STACK) {
+                    stk[sp++] = ch;
+                } else {
+                    overflow = true;
+                }
+            }
+        }
+    }
+    if (!FILL) {
+        ucnt[lf] = (int)nu;
+        wcnt[lf] = (int)nw;
+        const int64_t pb = pcount[b];
+        atomicAdd((unsigned long long*)&counts->p2p_pairs, (unsigned long long)(pb * upairs - pb));
+        atomicAdd((unsigned long long*)&counts->m2p_evals, (unsigned long long)(pb * nw));
+        atomicAdd((unsigned long long*)&counts->p2l_evals, (unsigned long long)(pb * nw));
+        if (overflow) atomicAdd((unsigned long long*)&counts->adj_mismatch, 1ull << 40);
+    }
+}
+
+// X = transpose of W: emit (w, leaf box) in leaf order, count members per box
+__global__ void k_x_emit(int nleaf, const int* leafbox, const int64_t* woff, const int* widx, uint32_t* xkey, uint32_t* xval,
+                         int* xcnt) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= nleaf) return;
+    const int b = leafbox[lf];
+    for (int64_t e = woff[lf]; e < woff[lf + 1]; ++e) {
+        xkey[e] = (uint32_t)widx[e];
+        xval[e] = (uint32_t)b;
+        atomicAdd(&xcnt[widx[e]], 1);
+    }
+}
+
+// M2L targets: boxes of level >= 2 keyed by their child octant
+__global__ void k_tgt_keys(int first, int nb, const int* coord, uint32_t* key, uint32_t* val) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb - first) return;
+    const int b = first + k;
+    key[k] = (uint32_t)((coord[3 * b] & 1) | ((coord[3 * b + 1] & 1) << 1) | ((coord[3 * b + 2] & 1) << 2));
+    val[k] = (uint32_t)b;
+}
+
+// padded per-octant layout of the M2L targets: every octant group starts on a
+// multiple of `tile`, so a tile never mixes octants
+__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int* gs) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int pad = 0;
+    for (int g = 0; g <= 8; ++g) {
+        int lo = 0, hi = ntgt;  // first index with key >= g
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)key[mid] < g) lo = mid + 1; else hi = mid;
+        }
+        gs[g] = lo;
+        gs[9 + g] = pad;
+        if (g < 8) {
+            int cnt_hi = ntgt, l2 = 0;  // first index with key >= g+1
+            int a = 0, b2 = ntgt;
+            while (a < b2) {
+                const int mid = (a + b2) >> 1;
+                if ((int)key[mid] < g + 1) a = mid + 1; else b2 = mid;
+            }
+            cnt_hi = a;
+            l2 = cnt_hi - lo;
+            pad += ((l2 + tile - 1) / tile) * tile;
+        }
+    }
+}
+__global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, uint32_t* pkey, uint32_t* pbox) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npad) return;
+    uint32_t k = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
+    for (int g = 0; g < 8; ++g) {
+        const int ps = gs[9 + g], pe = gs[9 + g + 1];
+        if (q >= ps && q < pe) {
+            const int local = q - ps;
+            if (local < gs[g + 1] - gs[g]) { k = (uint32_t)g; b = box[gs[g] + local]; }
+            break;
+        }
+    }
+    pkey[q] = k;
+    pbox[q] = b;
+}
+
+}  // namespace
+
+static inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
+static inline int bits_for(int64_t v) {
+    int b = 1;
+    while ((1ll << b) <= v) ++b;
+    return b;
+}
+
+int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) {
+    const cudaStream_t st = h.stream;
+    const int thr = h.prm.leaf_capacity;
+    DevCounts* dc;
+    RootInfo* root;
+    double* part;
+    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    OGX_TRY(arena_get(h.ws, S_ROOT, 1, &root));
+    const int nparts = 296;
+    OGX_TRY(arena_get(h.ws, S_BBOX, 6 * nparts, &part));
+    OGX_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCounts), st));
+
+    k_bbox_partial<<<nparts, 256, 0, st>>>(d_pos, n, part);
+    k_bbox_final<<<1, 32, 0, st>>>(part, nparts, h.prm.eps, root);
+
+    uint64_t* khi;
+    uint32_t *klo, *kidx;
+    OGX_TRY(arena_get(h.ws, S_KHI, n, &khi));
+    OGX_TRY(arena_get(h.ws, S_KLO, n, &klo));
+    OGX_TRY(arena_get(h.ws, S_IDX, n, &kidx));
+    k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi, klo, kidx);
+    OGX_TRY(radix_sort_key72(h, n, &khi, &klo, &kidx));
+
+    int *dfirst, *leaflev, *cnt, *leafflag, *leafstart, *level_off_dev;
+    signed char* cplthr;
+    int64_t *recoff, *leafscan;
+    OGX_TRY(arena_get(h.ws, S_TOPO_D, n, &dfirst));
+    OGX_TRY(arena_get(h.ws, S_TOPO_CPL, n, &cplthr));
+    OGX_TRY(arena_get(h.ws, S_TOPO_L, n, &leaflev));
+    OGX_TRY(arena_get(h.ws, S_TOPO_CNT, 2 * n + 64, &cnt));
+    leafflag = cnt + n + 32;
+    OGX_TRY(arena_get(h.ws, S_TOPO_COFF, 2 * (n + 1), &recoff));
+    leafscan = recoff + (n + 1);
+    OGX_TRY(arena_get(h.ws, S_LEAFSTART, n + 2 + kMaxDepth + 2, &leafstart));
+    level_off_dev = leafstart + n + 2;
+
+    k_topo_pairs<<<grid_for(n, 256), 256, 0, st>>>(khi, klo, n, thr, dfirst, cplthr);
+    const size_t wm_smem = WM_BLOCK + thr + 16;
+    if (wm_smem > 48 * 1024) {
+        OGX_CUDA(cudaFuncSetAttribute(k_topo_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wm_smem));
+    }
+    k_topo_levels<<<grid_for(n, WM_BLOCK), WM_BLOCK, wm_smem, st>>>(cplthr, dfirst, n, thr, root, leaflev, cnt, leafflag, dc);
+    OGX_TRY(scan_i32_to_i64(h, cnt, recoff, n));
+    OGX_TRY(scan_i32_to_i64(h, leafflag, leafscan, n));
+    k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev);
+    // sync point 1: box / leaf / level counts
+    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaStreamSynchronize(st));
+    const int nb = (int)h.h_counts->num_boxes;
+    const int nleaf = (int)h.h_counts->num_leaves;
+    h.max_level = h.h_counts->max_level;
+    h.level_off.assign(h.max_level + 2, 0);
+    for (int l = 0; l <= h.max_level; ++l) h.level_off[l + 1] = h.level_off[l] + h.h_counts->level_hist[l];
+
+    uint32_t *reckey, *recpos;
+    OGX_TRY(arena_get(h.ws, S_REC_KEY, nb, &reckey));
+    OGX_TRY(arena_get(h.ws, S_REC_POS, nb, &recpos));
+    k_emit_records<<<grid_for(n + 1, 256), 256, 0, st>>>(cnt, dfirst, leaflev, recoff, n, reckey, recpos, leafflag, leafscan,
+                                                          leafstart);
+    uint32_t *reclev, *recpos_s;
+    OGX_TRY(radix_sort_u32(h, S_REC_KEY, S_REC_POS, S_REC_KEY2, S_REC_POS2, nb, 5, &reclev, &recpos_s));
+
+    int *level, *coord, *parent, *child, *leafid, *pfirst, *pcount, *leafbox;
+    double* center;
+    OGX_TRY(arena_get(h.ws, S_BOX_LEVEL, nb, &level));
+    OGX_TRY(arena_get(h.ws, S_BOX_COORD, 3 * (size_t)nb, &coord));
+    OGX_TRY(arena_get(h.ws, S_BOX_CENTER, 4 * (size_t)nb, &center));
+    OGX_TRY(arena_get(h.ws, S_BOX_PARENT, nb, &parent));
+    OGX_TRY(arena_get(h.ws, S_BOX_CHILD, 8 * (size_t)nb, &child));
+    OGX_TRY(arena_get(h.ws, S_BOX_LEAFID, nb, &leafid));
+    OGX_TRY(arena_get(h.ws, S_BOX_PFIRST, nb, &pfirst));
+    OGX_TRY(arena_get(h.ws, S_BOX_PCOUNT, nb, &pcount));
+    OGX_TRY(arena_get(h.ws, S_LEAF_BOX, nleaf, &leafbox));
+    OGX_CUDA(cudaMemsetAsync(child, 0xFF, 8 * sizeof(int) * (size_t)nb, st));
+    OGX_CUDA(cudaMemsetAsync(pcount, 0, sizeof(int) * (size_t)nb, st));
+    k_boxes<<<grid_for(nb, 128), 128, 0, st>>>(nb, reclev, recpos_s, level_off_dev, khi, klo, leaflev, leafscan, leafstart, root,
+                                                level, coord, center, parent, child, leafid, pfirst, pcount, leafbox);
+    k_pcount_up<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, parent, pcount, dc);
+
+    // final body order: stable by leaf id from the original order
+    uint32_t *lk, *ident;
+    OGX_TRY(arena_get(h.ws, S_LEAFKEY, n, &lk));
+    OGX_TRY(arena_get(h.ws, S_PERM, n, &ident));
+    k_leafkey<<<grid_for(n, 256), 256, 0, st>>>(kidx, leafscan, n, lk, ident);
+    uint32_t *lk_s, *perm_s;
+    OGX_TRY(radix_sort_u32(h, S_LEAFKEY, S_PERM, S_LEAFKEY2, S_PERM2, n, bits_for(nleaf), &lk_s, &perm_s));
+    int* perm;
+    double *px, *py, *pz, *pm;
+    OGX_TRY(arena_get(h.ws, S_PERM_FINAL, n, &perm));
+    OGX_TRY(arena_get(h.ws, S_PX, n, &px));
+    OGX_TRY(arena_get(h.ws, S_PY, n, &py));
+    OGX_TRY(arena_get(h.ws, S_PZ, n, &pz));
+    OGX_TRY(arena_get(h.ws, S_PM, n, &pm));
+    k_gather_bodies<<<grid_for(n, 256), 256, 0, st>>>(perm_s, d_pos, d_mass, n, perm, px, py, pz, pm);
+    OGX_CUDA(cudaGetLastError());
+
+    TreeView& tv = h.tv;
+    tv.n = (int)n; tv.nb = nb; tv.nleaf = nleaf; tv.root = root;
+    tv.px = px; tv.py = py; tv.pz = pz; tv.pm = pm; tv.perm = perm;
+    tv.level = level; tv.coord = coord; tv.center = center; tv.parent = parent; tv.child = child;
+    tv.leafid = leafid; tv.pfirst = pfirst; tv.pcount = pcount; tv.leafbox = leafbox;
+    return OGX_OK;
+}
+
+int lists_build(Handle& h) {
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    const int nb = tv.nb, nleaf = tv.nleaf;
+    DevCounts* dc;
+    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    int* col;
+    OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
+    k_root_col<<<1, 32, 0, st>>>(col);
+    for (int l = 1; l <= h.max_level; ++l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - h.level_off[l];
+        if (count > 0)
+            k_colleagues<<<grid_for(count, 128), 128, 0, st>>>(first, count, tv.parent, tv.coord, tv.child, tv.center, tv.root,
+                                                                 col, dc);
+    }
+    tv.col = col;
+    int *ucnt, *wcnt;
+    int64_t *uoff, *woff;
+    OGX_TRY(arena_get(h.ws, S_U_CNT, nleaf, &ucnt));
+    OGX_TRY(arena_get(h.ws, S_W_CNT, nleaf, &wcnt));
+    OGX_TRY(arena_get(h.ws, S_U_OFF, nleaf + 1, &uoff));
+    OGX_TRY(arena_get(h.ws, S_W_OFF, nleaf + 1, &woff));
+    k_uw<false><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
+                                                     tv.root, ucnt, wcnt, nullptr, nullptr, nullptr, nullptr, dc);
+    OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
+    OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
+    // sync point 2: list sizes
+    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->u_total, uoff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->w_total, woff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaStreamSynchronize(st));
+    const int64_t nu = h.h_counts->u_total, nw = h.h_counts->w_total;
+    int *uidx, *widx;
+    OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
+    OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));
+    k_uw<true><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
+                                                    tv.root, nullptr, nullptr, uoff, woff, uidx, widx, dc);
+    tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
+
+    // X lists
+    uint32_t *xk, *xv;
+    int* xcnt;
+    int64_t* xoff;
+    OGX_TRY(arena_get(h.ws, S_X_KEY, nw + 1, &xk));
+    OGX_TRY(arena_get(h.ws, S_X_VAL, nw + 1, &xv));
+    OGX_TRY(arena_get(h.ws, S_X_CNT, nb, &xcnt));
+    OGX_TRY(arena_get(h.ws, S_X_OFF, nb + 1, &xoff));
+    OGX_CUDA(cudaMemsetAsync(xcnt, 0, sizeof(int) * (size_t)nb, st));
+    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt);
+    uint32_t *xk_s, *xv_s;
+    OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, bits_for(nb), &xk_s, &xv_s));
+    OGX_TRY(scan_i32_to_i64(h, xcnt, xoff, nb));
+    tv.x_off = xoff;
+    tv.x_idx = (const int*)xv_s;
+
+    // M2L targets grouped by child octant (levels >= 2)
+    const int first2 = (h.max_level >= 2) ? h.level_off[2] : nb;
+    const int ntgt = nb - first2;
+    uint32_t *tk, *tb;
+    OGX_TRY(arena_get(h.ws, S_TGT_KEY, ntgt + 1, &tk));
+    OGX_TRY(arena_get(h.ws, S_TGT_BOX, ntgt + 1, &tb));
+    if (ntgt > 0) {
+        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tk, tb);
+        uint32_t *tk_s, *tb_s;
+        OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 3, &tk_s, &tb_s));
+        h.tgt_key = tk_s;
+        h.tgt_box = tb_s;
+        const int tile = 64;
+        const int npad = ((ntgt + tile - 1) / tile + 8) * tile;
+        int* gs;
+        uint32_t *pk, *pb;
+        OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
+        OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
+        OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
+        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs);
+        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb);
+        h.tgt_tile_key = pk;
+        h.tgt_tile_box = pb;
+        h.ntgt_pad = npad;
+    } else {
+        h.ntgt_pad = 0;
+    }
+    h.ntgt = ntgt;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+}  // namespace ogx

@@ -1,0 +1,238 @@
+"""Python host binding of libogx.so (the C ABI in include/ogx.h).
+
+Mirrors the reference's solver interface (src3d/ForceSolver3D.hpp:20-28):
+
+    AdaptiveFMM3D(KernelParams3D{G, eps}, p, threshold)   -> AdaptiveFMM3D(G, eps, p, threshold)
+    DirectSolver3D(KernelParams3D{G, eps})                 -> DirectSolver3D(G, eps)
+    solver.computeAccelerations(bodies)                     -> solver.compute_accelerations(pos, mass)
+    solver.name()                                           -> solver.name()
+
+with numpy (n, 3) float64 positions in the original body order, exactly the
+memory of a ``std::vector<Vec3>``.  Every call goes through the compiled CUDA
+library; there is no CPU path here: if libogx.so is missing or the call fails,
+an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libogx.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NO_DEVICE, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_STATE = range(8)
+SOLVER_ADAPTIVE_FMM, SOLVER_DIRECT = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+# Every entry point declared in include/ogx.h (checked by the ABI test).
+EXPORTS = (
+    "ogx_params_default", "ogx_create", "ogx_destroy", "ogx_eval", "ogx_eval_device", "ogx_synchronize",
+    "ogx_name", "ogx_last_stats", "ogx_strerror", "ogx_last_error_message", "ogx_operator_matrix",
+    "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
+)
+
+
+class Params(C.Structure):
+    _fields_ = [("G", C.c_double), ("eps", C.c_double), ("p", C.c_int), ("leaf_capacity", C.c_int),
+                ("solver", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("stream", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n", C.c_int64), ("num_boxes", C.c_int32), ("num_leaves", C.c_int32),
+                ("max_leaf_occupancy", C.c_int32), ("max_level", C.c_int32),
+                ("list_u", C.c_int64), ("list_v", C.c_int64), ("list_w", C.c_int64), ("list_x", C.c_int64),
+                ("p2p_pairs", C.c_int64), ("m2p_evals", C.c_int64), ("p2l_evals", C.c_int64),
+                ("adjacency_mismatch", C.c_int64),
+                ("ms_tree", C.c_double), ("ms_lists", C.c_double), ("ms_upward", C.c_double), ("ms_m2l", C.c_double),
+                ("ms_p2l", C.c_double), ("ms_downward", C.c_double), ("ms_leaf", C.c_double), ("ms_total", C.c_double),
+                ("ms_h2d", C.c_double), ("ms_d2h", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class OgxError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        lib = load()
+        msg = lib.ogx_strerror(code).decode()
+        detail = lib.ogx_last_error_message().decode()
+        super().__init__(f"{what}: {msg} ({code}) {detail}".strip())
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libogx.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built (run `make -C on-galaxy_b200`)")
+    lib = C.CDLL(path)
+    vp, i64, dp, ip = C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    lib.ogx_params_default.argtypes = [C.POINTER(Params)]
+    lib.ogx_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+    lib.ogx_destroy.argtypes = [vp]
+    lib.ogx_eval.argtypes = [vp, i64, vp, vp, vp, vp]
+    lib.ogx_eval_device.argtypes = [vp, i64, vp, vp, vp, vp]
+    lib.ogx_synchronize.argtypes = [vp]
+    lib.ogx_name.argtypes = [vp]
+    lib.ogx_name.restype = C.c_char_p
+    lib.ogx_last_stats.argtypes = [vp, C.POINTER(Stats)]
+    lib.ogx_strerror.argtypes = [C.c_int]
+    lib.ogx_strerror.restype = C.c_char_p
+    lib.ogx_last_error_message.argtypes = []
+    lib.ogx_last_error_message.restype = C.c_char_p
+    lib.ogx_operator_matrix.argtypes = [C.c_int, C.c_int, C.c_int, dp]
+    lib.ogx_upload.argtypes = [vp, i64, vp, vp, vp]
+    lib.ogx_step.argtypes = [vp, C.c_double, C.c_int]
+    lib.ogx_download.argtypes = [vp, vp, vp, vp]
+    lib.ogx_tree_sizes.argtypes = [vp, C.POINTER(C.c_int64)]
+    lib.ogx_tree_boxes.argtypes = [vp, ip, dp, ip]
+    lib.ogx_tree_list.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), ip]
+    _lib = lib
+    return lib
+
+
+def _check(rc, what):
+    if rc != OK:
+        raise OgxError(rc, what)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def operator_matrix(kind: int, p: int, index: int) -> np.ndarray:
+    """Host-side translation matrix (kind 0=M2M, 1=L2L, 2=M2L), K x K with K=(p+1)^2."""
+    K = (p + 1) ** 2
+    out = np.zeros(K * K)
+    _check(load().ogx_operator_matrix(kind, p, index, out.ctypes.data_as(C.POINTER(C.c_double))),
+           "ogx_operator_matrix")
+    return out.reshape(K, K)
+
+
+class _Solver:
+    def __init__(self, G=1.0, eps=0.0, p=8, threshold=64, solver=SOLVER_ADAPTIVE_FMM, precision=PREC_FP64,
+                 device=0, stream=None):
+        lib = load()
+        prm = Params()
+        lib.ogx_params_default(C.byref(prm))
+        prm.G, prm.eps, prm.p, prm.leaf_capacity = float(G), float(eps), int(p), int(threshold)
+        prm.solver, prm.precision, prm.device = int(solver), int(precision), int(device)
+        prm.stream = stream
+        h = C.c_void_p()
+        _check(lib.ogx_create(C.byref(prm), C.byref(h)), "ogx_create")
+        self._h = h
+        self._lib = lib
+        self.params = prm
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ogx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def name(self) -> str:
+        return self._lib.ogx_name(self._h).decode()
+
+    def compute_accelerations(self, pos, mass, with_potential=False):
+        """ForceSolver3D::computeAccelerations on host arrays -> acc (n,3) [, pot (n,)]."""
+        pos = np.ascontiguousarray(pos, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64)
+        n = mass.shape[0]
+        if pos.shape != (n, 3):
+            raise ValueError("pos must be (n, 3)")
+        acc = np.zeros((n, 3))
+        pot = np.zeros(n) if with_potential else None
+        _check(self._lib.ogx_eval(self._h, n, _ptr(pos), _ptr(mass), _ptr(acc), _ptr(pot)), "ogx_eval")
+        return (acc, pot) if with_potential else acc
+
+    # torch-tensor (device) path: plumbing only, the tensors are plain device buffers
+    def compute_accelerations_device(self, pos_t, mass_t, acc_t, pot_t=None):
+        n = mass_t.shape[0]
+        _check(self._lib.ogx_eval_device(self._h, n, C.c_void_p(pos_t.data_ptr()), C.c_void_p(mass_t.data_ptr()),
+                                         C.c_void_p(acc_t.data_ptr()),
+                                         None if pot_t is None else C.c_void_p(pot_t.data_ptr())),
+               "ogx_eval_device")
+
+    def compute_accelerations_host_ptr(self, n, pos_p, mass_p, acc_p, pot_p=None):
+        """Host-buffer call on raw pointers (pinned buffers from torch)."""
+        _check(self._lib.ogx_eval(self._h, n, C.c_void_p(pos_p), C.c_void_p(mass_p), C.c_void_p(acc_p),
+                                  None if pot_p is None else C.c_void_p(pot_p)), "ogx_eval")
+
+    def synchronize(self):
+        _check(self._lib.ogx_synchronize(self._h), "ogx_synchronize")
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self._lib.ogx_last_stats(self._h, C.byref(s)), "ogx_last_stats")
+        return s.as_dict()
+
+    # device-resident leapfrog (VelocityVerlet3D)
+    def upload(self, pos, vel, mass):
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64)
+        _check(self._lib.ogx_upload(self._h, mass.shape[0], _ptr(pos), _ptr(vel), _ptr(mass)), "ogx_upload")
+        self._n = mass.shape[0]
+
+    def step(self, dt, nsteps=1):
+        _check(self._lib.ogx_step(self._h, float(dt), int(nsteps)), "ogx_step")
+
+    def download(self):
+        n = self._n
+        pos, vel, acc = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        _check(self._lib.ogx_download(self._h, _ptr(pos), _ptr(vel), _ptr(acc)), "ogx_download")
+        return pos, vel, acc
+
+    def tree(self):
+        """Tree of the last evaluation in the same layout as the oracle export."""
+        lib = self._lib
+        sizes = (C.c_int64 * 7)()
+        _check(lib.ogx_tree_sizes(self._h, sizes), "ogx_tree_sizes")
+        nb = int(sizes[0])
+        boxes = np.zeros((nb, 8), np.int32)
+        centers = np.zeros((nb, 4))
+        n = self.stats()["n"]
+        perm = np.zeros(max(n, 1), np.int32)
+        _check(lib.ogx_tree_boxes(self._h, boxes.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  centers.ctypes.data_as(C.POINTER(C.c_double)),
+                                  perm.ctypes.data_as(C.POINTER(C.c_int32))), "ogx_tree_boxes")
+        lists = {}
+        for k, name in enumerate(("colleague", "U", "V", "W", "X")):
+            off = np.zeros(nb + 1, np.int64)
+            idx = np.zeros(max(int(sizes[2 + k]), 1), np.int32)
+            _check(lib.ogx_tree_list(self._h, k, off.ctypes.data_as(C.POINTER(C.c_int64)),
+                                     idx.ctypes.data_as(C.POINTER(C.c_int32))), "ogx_tree_list")
+            lists[name] = (off, idx[: int(sizes[2 + k])])
+        return dict(boxes=boxes, centers=centers, perm=perm[:n], lists=lists, nleaf=int(sizes[1]))
+
+
+class AdaptiveFMM3D(_Solver):
+    """Drop-in for galaxy3d::AdaptiveFMM3D(KernelParams3D{G, eps}, p, threshold)."""
+
+    def __init__(self, G=1.0, eps=0.0, p=8, threshold=64, precision=PREC_FP64, device=0, stream=None):
+        super().__init__(G, eps, p, threshold, SOLVER_ADAPTIVE_FMM, precision, device, stream)
+
+
+class DirectSolver3D(_Solver):
+    """Drop-in for galaxy3d::DirectSolver3D(KernelParams3D{G, eps})."""
+
+    def __init__(self, G=1.0, eps=0.0, device=0, stream=None):
+        super().__init__(G, eps, 8, 64, SOLVER_DIRECT, PREC_FP64, device, stream)
