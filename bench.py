@@ -1,0 +1,335 @@
+"""Benchmark: adaptive-FMM force evaluation on the 1M-body two-galaxy merger.
+
+Workload (the configuration the headline metric is quoted on): two disk+bulge
+galaxies of 500,000 bodies each (80% exponential sech^2 disk, 20% Hernquist
+bulge), placed at x = -/+5 with relative velocity 0.5 along x and the second
+disk tilted by 30 degrees; velocities from the FP64 field (v_c^2 = -a_R R) plus
+0.1 v_c dispersion; p = 8, leaf capacity 64, G = 1, eps = 0.  One step = one
+device-resident leapfrog step with dt = 0.01 (drift, full force evaluation
+including tree build and lists, kick), as VelocityVerlet3D::step
+(src3d/Integrator3D.hpp:23-40).  Synthetic, seeded data.
+
+value   : bodies/s = N / (device time of one step), inputs resident in HBM, L2
+          flushed (256 MiB write) before every timed step, CUDA events per step.
+e2e     : bodies/s through the C ABI call that replaces
+          ForceSolver3D::computeAccelerations with host buffers (pinned), i.e.
+          H2D pos+mass, evaluation, D2H accelerations, every step.
+--impl reference : the reference's own CPU AdaptiveFMM3D (src3d headers compiled
+          into oracle/_ref) on a bounded sample of the same workload, all host
+          threads, one system per thread.
+Multi-GPU: replicas only (one independent merger per rank, no collective on the
+path); value = all ranks' bodies / max-over-ranks step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "on-galaxy_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "bodies/s, adaptive FMM 1M clustered @RMS err≤1e-5 vs FP64 form; p99 step ms"
+N_PER = 500_000
+P_ORDER = 8
+THR = 64
+DT = 0.01
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--n-per", type=int, default=N_PER)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- reference arm
+def cpu_sample_bodies(n_per, seed):
+    import ogx_ic
+    pos, _, mass, _ = ogx_ic.merger(n_per, seed=seed, accel_fn=None)
+    return pos, mass
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO, Oracle, Reference
+
+    threads = os.cpu_count() or 1
+    n_per = 4096  # 8,192-body merger per system, same generator as the workload
+    kind = "reference" if os.path.exists(REF_SO) else "port"
+    samples = [cpu_sample_bodies(n_per, seed=100 + s) for s in range(threads)]
+    pos = np.stack([s[0] for s in samples])
+    mass = np.stack([s[1] for s in samples])
+    if kind == "reference":
+        lib = Reference()
+        run = lambda: lib.adaptive_fmm_batch(pos, mass, 1.0, 0.0, P_ORDER, THR, threads)  # noqa: E731
+    else:
+        orc = Oracle()
+        run = lambda: [orc.adaptive_fmm(pos[s], mass[s], p=P_ORDER, thr=THR, with_pot=False)  # noqa: E731
+                       for s in range(threads)]
+    for _ in range(args.warmup):
+        run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    n_tot = pos.shape[0] * pos.shape[1]
+    ms = 1e3 * float(np.mean(times))
+    value = n_tot / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "two-galaxy merger (disk+bulge), one force evaluation per system", "p": P_ORDER,
+                   "leaf_capacity": THR, "n_per_system": int(pos.shape[1]), "systems_per_step": threads},
+        "p50_step_ms": 1e3 * float(np.percentile(times, 50)), "p99_step_ms": 1e3 * float(np.percentile(times, 99)),
+        "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": threads, "kind": kind,
+                         "sample": f"{threads} independent {pos.shape[1]}-body mergers per step, AdaptiveFMM3D "
+                                   f"p={P_ORDER} thr={THR}, one per thread"},
+        "e2e": {"value": value, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_single():
+    """Reference CPU AdaptiveFMM3D on one core, bounded sample (16,384-body merger, one evaluation)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import REF_SO, Oracle, Reference
+    pos, mass = cpu_sample_bodies(8192, seed=100)
+    kind = "reference" if os.path.exists(REF_SO) else "port"
+    t0 = time.perf_counter()
+    if kind == "reference":
+        Reference().adaptive_fmm(pos, mass, p=P_ORDER, thr=THR)
+    else:
+        Oracle().adaptive_fmm(pos, mass, p=P_ORDER, thr=THR, with_pot=False)
+    sec = time.perf_counter() - t0
+    return {"value": pos.shape[0] / sec, "unit": "bodies/s", "cores": 1, "kind": kind,
+            "sample": f"one AdaptiveFMM3D evaluation of a {pos.shape[0]}-body merger (2x{pos.shape[0] // 2}, same "
+                      f"generator), p={P_ORDER}, thr={THR}, {sec:.1f} s on 1 core; box has {os.cpu_count()} cores"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/ogx_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.out, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.out).read().strip().splitlines()]
+            rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import ogx
+    import ogx_ic
+
+    # a dedicated stream: the library and the timing events must share it (the legacy
+    # default stream has handle 0, which the library would replace by its own stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    prec = ogx.PREC_MIXED if args.precision == "mixed" else ogx.PREC_FP64
+    # ---- initial conditions (untimed): FP64 field for the circular velocities
+    with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as ic_solver:
+        pos, vel, mass, _ = ogx_ic.merger(args.n_per, seed=1, accel_fn=ic_solver.compute_accelerations)
+    n = mass.shape[0]
+    try:
+        solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local,
+                                   stream=stream.cuda_stream)
+        solver.upload(pos, vel, mass)
+    except ogx.OgxError as e:
+        if e.code != ogx.ERR_UNSUPPORTED:
+            raise
+        prec = ogx.PREC_FP64
+        solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local, stream=stream.cuda_stream)
+        solver.upload(pos, vel, mass)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+        solver.step(DT, 1)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    phase = []
+    barrier()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            solver.step(DT, 1)
+            ends[k].record(stream)
+            phase.append(solver.stats())
+        barrier()
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    my_ms = float(step_ms.sum())
+    tot_ms = my_ms
+    if dist is not None:
+        t = torch.tensor([my_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    ms_per_step = tot_ms / args.steps
+    value = world * n / (ms_per_step / 1e3)
+    st = phase[-1]
+
+    # ---- e2e through the C ABI with pinned host buffers
+    pos_h = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
+    mass_h = torch.from_numpy(np.ascontiguousarray(mass)).pin_memory()
+    acc_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        solver.compute_accelerations_host_ptr(n, pos_h.data_ptr(), mass_h.data_ptr(), acc_h.data_ptr())
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solver.compute_accelerations_host_ptr(n, pos_h.data_ptr(), mass_h.data_ptr(), acc_h.data_ptr())
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_mean = float(np.mean(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([e2e_mean], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+
+    # ---- accuracy on the evaluated configuration (untimed)
+    acc_info = {}
+    if not args.no_accuracy and rank == 0:
+        acc_form = acc_h.numpy().copy()
+        with ogx.DirectSolver3D(device=local) as d:
+            ref = d.compute_accelerations(pos, mass)
+        with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as f64:
+            acc64 = f64.compute_accelerations(pos, mass)
+
+        def errs(r, g):
+            a = np.linalg.norm(r, axis=1)
+            e = np.linalg.norm(g - r, axis=1)
+            return float(np.sqrt((e * e).sum() / (a * a).sum())), float(np.max(e / np.maximum(a, 1e-6 * a.max())))
+        rms, mx = errs(ref, acc_form)
+        rms64, mx64 = errs(ref, acc64)
+        rmsf, _ = errs(acc64, acc_form)
+        acc_info = {"rms_vs_fp64_direct": rms, "max_rel_vs_fp64_direct": mx, "rms_fp64_form_vs_direct": rms64,
+                    "max_rel_fp64_form_vs_direct": mx64, "rms_vs_fp64_form": rmsf}
+
+    # ---- roofline of the dominant phase (CUDA events inside the library, same stream)
+    phases = {k: float(np.mean([p[k] for p in phase])) for k in
+              ("ms_tree", "ms_lists", "ms_upward", "ms_m2l", "ms_p2l", "ms_downward", "ms_leaf", "ms_total")}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    tc_peak = peaks.get("bf16_tflops", 1590.0)
+    K = (P_ORDER + 1) ** 2
+    m2l_flops = 2.0 * K * K * st["list_v"] if st["list_v"] else 0.0
+    roofline = {"kernel": "m2l", "bound": "tensor" if prec == ogx.PREC_MIXED else "fp64",
+                "achieved": (m2l_flops / (phases["ms_m2l"] / 1e3) / 1e12) if phases["ms_m2l"] > 0 else None,
+                "peak": tc_peak, "unit": "TFLOP/s", "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1.59 PFLOP/s"}
+    if roofline["achieved"] is not None:
+        roofline["frac"] = roofline["achieved"] / roofline["peak"]
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "mixed(f32 P2P, 3xTF32 M2L, f64 translations)" if prec == ogx.PREC_MIXED else "f64",
+        "data": "synthetic",
+        "config": {"workload": f"two-galaxy merger, {n} bodies (2x{args.n_per} disk+bulge), one leapfrog step dt=0.01",
+                   "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
+        "e2e": {"value": world * n / (e2e_mean / 1e3), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
+                "d2h_bytes_per_step": int(24 * n), "ms_per_step": e2e_mean},
+        "phases_ms": phases, "tree": {k: st[k] for k in ("num_boxes", "num_leaves", "max_level", "max_leaf_occupancy",
+                                                          "list_u", "list_v", "list_w", "p2p_pairs", "m2p_evals")},
+        "pair_interactions_per_s": st["p2p_pairs"] * world / (ms_per_step / 1e3),
+        "roofline": roofline, "accuracy": acc_info, "clocks": clk.summary(),
+        "gpu_launches": int(st.get("launches", 0)) * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_single()
+    solver.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

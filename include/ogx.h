@@ -73,6 +73,7 @@ typedef struct {
     int64_t adjacency_mismatch;/* integer vs FP64 adjacency disagreements (0 expected) */
     double ms_tree, ms_lists, ms_upward, ms_m2l, ms_p2l, ms_downward, ms_leaf, ms_total;
     double ms_h2d, ms_d2h;     /* host-buffer calls only */
+    int64_t launches;          /* kernels launched by the last evaluation (+ drift/kick in ogx_step) */
 } ogx_stats;
 
 /* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0. */

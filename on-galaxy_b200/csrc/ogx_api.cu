@@ -147,11 +147,13 @@ static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* 
     std::memset(&h.stats, 0, sizeof(h.stats));
     h.stats.n = n;
     if (n == 0) return OGX_OK;
+    const int64_t l0 = h.launches;
     const cudaStream_t st = h.stream;
     OGX_CUDA(cudaEventRecord(h.ev[0], st));
     if (h.prm.solver == OGX_SOLVER_DIRECT) {
         OGX_TRY(direct_eval(h, d_pos, d_mass, n, d_acc, d_pot, false));
         OGX_CUDA(cudaEventRecord(h.ev[8], st));
+        h.stats.launches = h.launches - l0;
         return OGX_OK;
     }
     OGX_TRY(ensure_operator_tables(h));
@@ -175,6 +177,8 @@ static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* 
     h.stats.m2p_evals = c.m2p_evals;
     h.stats.p2l_evals = c.p2l_evals;
     h.stats.adjacency_mismatch = c.adj_mismatch;
+    h.stats.list_v = c.v_total;
+    h.stats.launches = h.launches - l0;
     return OGX_OK;
 }
 
@@ -362,6 +366,7 @@ int ogx_upload(void* handle, int64_t n, const double* pos, const double* vel, co
     OGX_CUDA(cudaMemcpyAsync(dv, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
     OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
     OGX_TRY(eval_device(h, n, dp, dm, da, nullptr));  // VelocityVerlet3D::initialize
+    finish_stats(h);
     h.resident = true;
     h.n = n;
     return OGX_OK;
@@ -381,10 +386,11 @@ int ogx_step(void* handle, double dt, int nsteps) {
     OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
     const int grid = (int)((n3 + 255) / 256);
     for (int s = 0; s < nsteps; ++s) {
-        k_drift<<<grid, 256, 0, h.stream>>>(dp, dv, da, n3, dt, 0.5 * dt * dt);
+        k_drift<<<grid, 256, 0, h.stream>>>(dp, dv, da, n3, dt, 0.5 * dt * dt); ++h.launches;
         OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
-        k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt);
+        k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt); ++h.launches;
         OGX_CUDA(cudaMemcpyAsync(da, dn, n3 * sizeof(double), cudaMemcpyDeviceToDevice, h.stream));
+        h.stats.launches += 2;  // drift + kick around the evaluation
     }
     OGX_CUDA(cudaGetLastError());
     h.n = n;

@@ -74,11 +74,11 @@ int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n,
     const int grid = (int)((n + DT - 1) / DT);
     const double eps2 = h.prm.eps * h.prm.eps;
     if (fp32) {
-        if (d_pot) k_direct<float, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, d_pot);
-        else k_direct<float, false><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, nullptr);
+        if (d_pot) { k_direct<float, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, d_pot); ++h.launches; }
+        else { k_direct<float, false><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, nullptr); ++h.launches; }
     } else {
-        if (d_pot) k_direct<double, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, d_pot);
-        else k_direct<double, false><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, nullptr);
+        if (d_pot) { k_direct<double, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, d_pot); ++h.launches; }
+        else { k_direct<double, false><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, nullptr); ++h.launches; }
     }
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;

@@ -376,10 +376,10 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     const size_t p2x_smem = 4 * 32 * LD * sizeof(double);
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
-    k_p2x<P, 0><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M);
+    k_p2x<P, 0><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
     for (int l = h.max_level - 1; l >= 0; --l) {
         const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr);
+        if (count > 0) { k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
     }
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
     // M2L
@@ -388,25 +388,25 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
         const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
         OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
         const int ntiles = h.ntgt_pad / M2L_TGT;
-        k_m2l_fp64<P><<<ntiles, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M, Lown);
+        k_m2l_fp64<P><<<ntiles, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M, Lown); ++h.launches;
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));
     // P2L
-    k_p2x<P, 1><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown);
+    k_p2x<P, 1><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
     // L2L top-down
     for (int l = 0; l <= h.max_level; ++l) {
         const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown);
+        if (count > 0) { k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
     }
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     // leaves
     const bool pot = d_pot != nullptr;
-    if (pot) k_leaf_far<P, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far);
-    else k_leaf_far<P, false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far);
+    if (pot) { k_leaf_far<P, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    else { k_leaf_far<P, false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
-    if (pot) k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot);
-    else k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr);
+    if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
+    else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[7], st));
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;

@@ -113,6 +113,7 @@ struct DevCounts {
     int64_t u_total, w_total;
     int64_t p2p_pairs, m2p_evals, p2l_evals;
     int64_t adj_mismatch;
+    int64_t v_total;
     int32_t nonleaf_level[kMaxDepth + 2];
 };
 
@@ -150,6 +151,7 @@ struct Handle {
     double* h_stage = nullptr;      // pinned staging for host-buffer calls
     size_t h_stage_cap = 0;
     ogx_stats stats{};
+    int64_t launches = 0;            // kernels launched by this handle (running total)
     std::vector<int32_t> level_off;  // host copy of level offsets (num levels + 1)
     int max_level = 0;
     int64_t n = 0;

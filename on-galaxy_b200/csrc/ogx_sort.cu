@@ -236,9 +236,9 @@ int scan_i32_to_i64(Handle& h, const int* in, int64_t* out, int64_t n) {
         OGX_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), h.stream));
         return OGX_OK;
     }
-    sc_partials<<<nparts, SC_THREADS, 0, h.stream>>>(in, n, part);
-    sc_scan_partials<<<1, SC_THREADS, 0, h.stream>>>(part, nparts);
-    sc_finish<<<nparts, SC_THREADS, 0, h.stream>>>(in, n, part, out, nparts);
+    sc_partials<<<nparts, SC_THREADS, 0, h.stream>>>(in, n, part); ++h.launches;
+    sc_scan_partials<<<1, SC_THREADS, 0, h.stream>>>(part, nparts); ++h.launches;
+    sc_finish<<<nparts, SC_THREADS, 0, h.stream>>>(in, n, part, out, nparts); ++h.launches;
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
@@ -251,9 +251,9 @@ static int radix_passes(Handle& h, KO a, KO b, uint32_t* va, uint32_t* vb, int64
     KO src = a, dst = b;
     uint32_t *vs = va, *vd = vb;
     for (int pass = 0; pass < npasses; ++pass) {
-        rs_hist<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, n, pass, hist, nblocks);
-        rs_scan<<<1, 1024, 0, h.stream>>>(hist, (int64_t)256 * nblocks);
-        rs_scatter<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, dst, vs, vd, n, pass, hist, nblocks);
+        rs_hist<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, n, pass, hist, nblocks); ++h.launches;
+        rs_scan<<<1, 1024, 0, h.stream>>>(hist, (int64_t)256 * nblocks); ++h.launches;
+        rs_scatter<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, dst, vs, vd, n, pass, hist, nblocks); ++h.launches;
         std::swap(src, dst);
         std::swap(vs, vd);
     }

@@ -315,7 +315,7 @@ __global__ void k_colleagues(int first, int count, const int* parent, const int*
 #pragma unroll
     for (int d = 0; d < 27; ++d) mine[d] = -1;
     const double tol = root->tol;
-    int mism = 0;
+    int mism = 0, nv = 0;
     for (int D = 0; D < 27; ++D) {
         const int Q = col[27 * P + D];
         if (Q < 0) continue;
@@ -326,12 +326,14 @@ __global__ void k_colleagues(int first, int count, const int* parent, const int*
             const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
             const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
             if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
+            nv += !adj_i;
             if (adj_i) mine[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] = c;
         }
     }
 #pragma unroll
     for (int d = 0; d < 27; ++d) col[27 * b + d] = mine[d];
     if (mism) atomicAdd((unsigned long long*)&counts->adj_mismatch, (unsigned long long)mism);
+    if (nv) atomicAdd((unsigned long long*)&counts->v_total, (unsigned long long)nv);
 }
 
 constexpr int UW_STACK = 256;
@@ -487,15 +489,15 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_TRY(arena_get(h.ws, S_BBOX, 6 * nparts, &part));
     OGX_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCounts), st));
 
-    k_bbox_partial<<<nparts, 256, 0, st>>>(d_pos, n, part);
-    k_bbox_final<<<1, 32, 0, st>>>(part, nparts, h.prm.eps, root);
+    k_bbox_partial<<<nparts, 256, 0, st>>>(d_pos, n, part); ++h.launches;
+    k_bbox_final<<<1, 32, 0, st>>>(part, nparts, h.prm.eps, root); ++h.launches;
 
     uint64_t* khi;
     uint32_t *klo, *kidx;
     OGX_TRY(arena_get(h.ws, S_KHI, n, &khi));
     OGX_TRY(arena_get(h.ws, S_KLO, n, &klo));
     OGX_TRY(arena_get(h.ws, S_IDX, n, &kidx));
-    k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi, klo, kidx);
+    k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi, klo, kidx); ++h.launches;
     OGX_TRY(radix_sort_key72(h, n, &khi, &klo, &kidx));
 
     int *dfirst, *leaflev, *cnt, *leafflag, *leafstart, *level_off_dev;
@@ -511,15 +513,15 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_TRY(arena_get(h.ws, S_LEAFSTART, n + 2 + kMaxDepth + 2, &leafstart));
     level_off_dev = leafstart + n + 2;
 
-    k_topo_pairs<<<grid_for(n, 256), 256, 0, st>>>(khi, klo, n, thr, dfirst, cplthr);
+    k_topo_pairs<<<grid_for(n, 256), 256, 0, st>>>(khi, klo, n, thr, dfirst, cplthr); ++h.launches;
     const size_t wm_smem = WM_BLOCK + thr + 16;
     if (wm_smem > 48 * 1024) {
         OGX_CUDA(cudaFuncSetAttribute(k_topo_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wm_smem));
     }
-    k_topo_levels<<<grid_for(n, WM_BLOCK), WM_BLOCK, wm_smem, st>>>(cplthr, dfirst, n, thr, root, leaflev, cnt, leafflag, dc);
+    k_topo_levels<<<grid_for(n, WM_BLOCK), WM_BLOCK, wm_smem, st>>>(cplthr, dfirst, n, thr, root, leaflev, cnt, leafflag, dc); ++h.launches;
     OGX_TRY(scan_i32_to_i64(h, cnt, recoff, n));
     OGX_TRY(scan_i32_to_i64(h, leafflag, leafscan, n));
-    k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev);
+    k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev); ++h.launches;
     // sync point 1: box / leaf / level counts
     OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaStreamSynchronize(st));
@@ -533,7 +535,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_TRY(arena_get(h.ws, S_REC_KEY, nb, &reckey));
     OGX_TRY(arena_get(h.ws, S_REC_POS, nb, &recpos));
     k_emit_records<<<grid_for(n + 1, 256), 256, 0, st>>>(cnt, dfirst, leaflev, recoff, n, reckey, recpos, leafflag, leafscan,
-                                                          leafstart);
+                                                          leafstart); ++h.launches;
     uint32_t *reclev, *recpos_s;
     OGX_TRY(radix_sort_u32(h, S_REC_KEY, S_REC_POS, S_REC_KEY2, S_REC_POS2, nb, 5, &reclev, &recpos_s));
 
@@ -551,14 +553,14 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_CUDA(cudaMemsetAsync(child, 0xFF, 8 * sizeof(int) * (size_t)nb, st));
     OGX_CUDA(cudaMemsetAsync(pcount, 0, sizeof(int) * (size_t)nb, st));
     k_boxes<<<grid_for(nb, 128), 128, 0, st>>>(nb, reclev, recpos_s, level_off_dev, khi, klo, leaflev, leafscan, leafstart, root,
-                                                level, coord, center, parent, child, leafid, pfirst, pcount, leafbox);
-    k_pcount_up<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, parent, pcount, dc);
+                                                level, coord, center, parent, child, leafid, pfirst, pcount, leafbox); ++h.launches;
+    k_pcount_up<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, parent, pcount, dc); ++h.launches;
 
     // final body order: stable by leaf id from the original order
     uint32_t *lk, *ident;
     OGX_TRY(arena_get(h.ws, S_LEAFKEY, n, &lk));
     OGX_TRY(arena_get(h.ws, S_PERM, n, &ident));
-    k_leafkey<<<grid_for(n, 256), 256, 0, st>>>(kidx, leafscan, n, lk, ident);
+    k_leafkey<<<grid_for(n, 256), 256, 0, st>>>(kidx, leafscan, n, lk, ident); ++h.launches;
     uint32_t *lk_s, *perm_s;
     OGX_TRY(radix_sort_u32(h, S_LEAFKEY, S_PERM, S_LEAFKEY2, S_PERM2, n, bits_for(nleaf), &lk_s, &perm_s));
     int* perm;
@@ -568,7 +570,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_TRY(arena_get(h.ws, S_PY, n, &py));
     OGX_TRY(arena_get(h.ws, S_PZ, n, &pz));
     OGX_TRY(arena_get(h.ws, S_PM, n, &pm));
-    k_gather_bodies<<<grid_for(n, 256), 256, 0, st>>>(perm_s, d_pos, d_mass, n, perm, px, py, pz, pm);
+    k_gather_bodies<<<grid_for(n, 256), 256, 0, st>>>(perm_s, d_pos, d_mass, n, perm, px, py, pz, pm); ++h.launches;
     OGX_CUDA(cudaGetLastError());
 
     TreeView& tv = h.tv;
@@ -587,12 +589,12 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
     int* col;
     OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
-    k_root_col<<<1, 32, 0, st>>>(col);
+    k_root_col<<<1, 32, 0, st>>>(col); ++h.launches;
     for (int l = 1; l <= h.max_level; ++l) {
         const int first = h.level_off[l], count = h.level_off[l + 1] - h.level_off[l];
         if (count > 0)
             k_colleagues<<<grid_for(count, 128), 128, 0, st>>>(first, count, tv.parent, tv.coord, tv.child, tv.center, tv.root,
-                                                                 col, dc);
+                                                                 col, dc); ++h.launches;
     }
     tv.col = col;
     int *ucnt, *wcnt;
@@ -602,7 +604,7 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_U_OFF, nleaf + 1, &uoff));
     OGX_TRY(arena_get(h.ws, S_W_OFF, nleaf + 1, &woff));
     k_uw<false><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
-                                                     tv.root, ucnt, wcnt, nullptr, nullptr, nullptr, nullptr, dc);
+                                                     tv.root, ucnt, wcnt, nullptr, nullptr, nullptr, nullptr, dc); ++h.launches;
     OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
     OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
     // sync point 2: list sizes
@@ -615,7 +617,7 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
     OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));
     k_uw<true><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
-                                                    tv.root, nullptr, nullptr, uoff, woff, uidx, widx, dc);
+                                                    tv.root, nullptr, nullptr, uoff, woff, uidx, widx, dc); ++h.launches;
     tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
 
     // X lists
@@ -627,7 +629,7 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_X_CNT, nb, &xcnt));
     OGX_TRY(arena_get(h.ws, S_X_OFF, nb + 1, &xoff));
     OGX_CUDA(cudaMemsetAsync(xcnt, 0, sizeof(int) * (size_t)nb, st));
-    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt);
+    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt); ++h.launches;
     uint32_t *xk_s, *xv_s;
     OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, bits_for(nb), &xk_s, &xv_s));
     OGX_TRY(scan_i32_to_i64(h, xcnt, xoff, nb));
@@ -641,7 +643,7 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_TGT_KEY, ntgt + 1, &tk));
     OGX_TRY(arena_get(h.ws, S_TGT_BOX, ntgt + 1, &tb));
     if (ntgt > 0) {
-        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tk, tb);
+        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tk, tb); ++h.launches;
         uint32_t *tk_s, *tb_s;
         OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 3, &tk_s, &tb_s));
         h.tgt_key = tk_s;
@@ -653,8 +655,8 @@ int lists_build(Handle& h) {
         OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
         OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
         OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
-        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs);
-        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb);
+        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs); ++h.launches;
+        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb); ++h.launches;
         h.tgt_tile_key = pk;
         h.tgt_tile_box = pb;
         h.ntgt_pad = npad;
