@@ -141,6 +141,8 @@ __global__ void k_kick(double* vel, const double* acc_old, const double* acc_new
     if (i < n3) vel[i] += (acc_old[i] + acc_new[i]) * half_dt;
 }
 
+static int device_error(Handle& h);
+
 static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
     h.n = n;
     h.tree_valid = false;
@@ -148,6 +150,7 @@ static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* 
     h.stats.n = n;
     if (n == 0) return OGX_OK;
     const int64_t l0 = h.launches;
+    OGX_TRY(device_error(h));
     const cudaStream_t st = h.stream;
     OGX_CUDA(cudaEventRecord(h.ev[0], st));
     if (h.prm.solver == OGX_SOLVER_DIRECT) {
@@ -179,6 +182,16 @@ static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* 
     h.stats.adjacency_mismatch = c.adj_mismatch;
     h.stats.list_v = c.v_total;
     h.stats.launches = h.launches - l0;
+    return OGX_OK;
+}
+
+// a bounded device wait that ran out in the previous evaluation (read after a sync)
+static int device_error(Handle& h) {
+    if (h.h_err && *h.h_err) {
+        *h.h_err = 0;
+        set_last_error(OGX_ERR_TIMEOUT, "a bounded device wait ran out (tensor-core M2L pipeline)");
+        return OGX_ERR_TIMEOUT;
+    }
     return OGX_OK;
 }
 
@@ -265,6 +278,8 @@ int ogx_create(const ogx_params* prm, void** handle) {
         h->own_stream = true;
     }
     OGX_CUDA(cudaMallocHost(&h->h_counts, sizeof(DevCounts)));
+    OGX_CUDA(cudaMallocHost(&h->h_err, sizeof(int)));
+    *h->h_err = 0;
     std::memset(h->h_counts, 0, sizeof(DevCounts));
     for (auto& e : h->ev) OGX_CUDA(cudaEventCreate(&e));
     *handle = h.release();
@@ -279,6 +294,7 @@ int ogx_destroy(void* handle) {
         cudaStreamSynchronize(h->stream);
         h->ws.release();
         if (h->h_counts) cudaFreeHost(h->h_counts);
+        if (h->h_err) cudaFreeHost(h->h_err);
         if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto& e : h->ev)
             if (e) cudaEventDestroy(e);
@@ -308,6 +324,7 @@ int ogx_synchronize(void* handle) {
     HANDLE(handle);
     DeviceGuard g(h.device);
     OGX_CUDA(cudaStreamSynchronize(h.stream));
+    OGX_TRY(device_error(h));
     return OGX_OK;
 }
 
@@ -337,6 +354,7 @@ int ogx_eval(void* handle, int64_t n, const double* pos, const double* mass, dou
     if (pot) OGX_CUDA(cudaMemcpyAsync(pot, dpot, n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
     OGX_CUDA(cudaEventRecord(e1, h.stream));
     OGX_CUDA(cudaStreamSynchronize(h.stream));
+    OGX_TRY(device_error(h));
     finish_stats(h);
     h.stats.ms_h2d = h2d;
     h.stats.ms_d2h = ev_ms(e0, e1);

@@ -18,78 +18,19 @@
 //   leaf near     warp per leaf: softened P2P over the U list, j != i (:95-103),
 //                 then acc[orig] = G (far + near) (:104)
 // Potentials (pot = -G Phi) are produced alongside when requested.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
 #include "ogx_harmonics.cuh"
+#include "ogx_expansion_kernels.cuh"
+#include "ogx_mixed_kernels.cuh"
 
 namespace ogx {
 
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-
-// ---- P2M / P2L: particle -> expansion --------------------------------------------
-// MODE 0: P2M for leaf `lf`: coefficients q conj(R(u)), u = (x - c)/side, store.
-// MODE 1: P2L for box `b` over X(b): (q/side) conj(S(u)), accumulate.
-template <int P, int MODE>
-__global__ void __launch_bounds__(128) k_p2x(TreeView tv, int ntargets, double* out) {
-    constexpr int K = (P + 1) * (P + 1);
-    constexpr int LD = K | 1;
-    extern __shared__ double s_buf[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int t = blockIdx.x * 4 + wid;
-    if (t >= ntargets) return;
-    double* buf = s_buf + (size_t)wid * 32 * LD;
-    const int b = (MODE == 0) ? tv.leafbox[t] : t;
-    int64_t e0, e1;
-    if (MODE == 0) { e0 = 0; e1 = 1; }
-    else { e0 = tv.x_off[b]; e1 = tv.x_off[b + 1]; if (e0 == e1) return; }
-    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
-    const double side = 2.0 * tv.center[4 * b + 3], inv = 1.0 / side;
-    constexpr int NPL = (K + 31) / 32;
-    double acc[NPL];
-#pragma unroll
-    for (int q = 0; q < NPL; ++q) acc[q] = 0.0;
-    for (int64_t e = e0; e < e1; ++e) {
-        const int src = (MODE == 0) ? b : tv.x_idx[e];
-        const int f0 = tv.pfirst[src], cnt = tv.pcount[src];
-        for (int j0 = 0; j0 < cnt; j0 += 32) {
-            const int j = j0 + lane;
-            double* row = buf + (size_t)lane * LD;
-            if (j < cnt) {
-                const int i = f0 + j;
-                const double q = tv.pm[i];
-                const double ux = (tv.px[i] - cx) * inv, uy = (tv.py[i] - cy) * inv, uz = (tv.pz[i] - cz) * inv;
-                auto put = [&](int n, int m, double re, double im) {
-                    if (m == 0) row[n * n] = q * re;
-                    else { row[n * n + 2 * m - 1] = q * re; row[n * n + 2 * m] = -q * im; }
-                };
-                if (MODE == 0) for_regular<P>(ux, uy, uz, put);
-                else for_singular<P>(ux, uy, uz, put);
-            } else {
-                for (int d = 0; d < K; ++d) row[d] = 0.0;
-            }
-            __syncwarp();
-#pragma unroll
-            for (int q = 0; q < NPL; ++q) {
-                const int d = lane + 32 * q;
-                if (d < K) {
-                    double s = 0.0;
-#pragma unroll 8
-                    for (int r = 0; r < 32; ++r) s += buf[(size_t)r * LD + d];
-                    acc[q] += s;
-                }
-            }
-            __syncwarp();
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < NPL; ++q) {
-        const int d = lane + 32 * q;
-        if (d < K) {
-            if (MODE == 0) out[(size_t)b * K + d] = acc[q];
-            else out[(size_t)b * K + d] += acc[q] * inv;
-        }
-    }
-}
 
 // ---- M2M (MODE 0) / L2L (MODE 1) for the boxes of one level -----------------------
 // Matrices are stored transposed (k-major) so lanes over output rows coalesce.
@@ -240,85 +181,6 @@ __global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uin
     }
 }
 
-// ---- leaf far field: L2P + W-list M2P ---------------------------------------------------
-template <int P, bool POT>
-__global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const double* mpole, const double* local, double* far) {
-    constexpr int K = (P + 1) * (P + 1);
-    constexpr int KG = P * P;               // local gradient: degree P-1
-    constexpr int KH = (P + 2) * (P + 2);   // multipole gradient: degree P+1
-    __shared__ double s_c[4][K];
-    __shared__ double s_g[4][3][KH];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int lf = blockIdx.x * 4 + wid;
-    if (lf >= tv.nleaf) return;
-    const int b = tv.leafbox[lf];
-    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
-    const double side = 2.0 * tv.center[4 * b + 3], inv = 1.0 / side;
-    for (int j0 = 0; j0 < cnt; j0 += 32) {
-        const int j = j0 + lane;
-        const bool act = j < cnt;
-        const int i = f0 + (act ? j : 0);
-        const double x = tv.px[i], y = tv.py[i], z = tv.pz[i];
-        double gx = 0, gy = 0, gz = 0, phi = 0;
-        // L2P
-        for (int d = lane; d < K; d += 32) s_c[wid][d] = local[(size_t)b * K + d];
-        __syncwarp();
-        for (int d = lane; d < KG; d += 32) {
-            double g[3];
-            local_grad_dof(s_c[wid], d, g);
-            s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
-        }
-        __syncwarp();
-        {
-            const double ux = (x - cx) * inv, uy = (y - cy) * inv, uz = (z - cz) * inv;
-            double ax = 0, ay = 0, az = 0, ph = 0;
-            for_regular<P>(ux, uy, uz, [&](int n, int m, double re, double im) {
-                const double w = (m == 0) ? 1.0 : 2.0;
-                const int dr = dof_re(n, m);
-                if (POT) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : 0.0));
-                if (n < P) {
-                    ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : 0.0));
-                    ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : 0.0));
-                    az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : 0.0));
-                }
-            });
-            gx = ax * inv; gy = ay * inv; gz = az * inv; phi = ph;
-        }
-        __syncwarp();
-        // M2P over W(b)
-        for (int64_t e = tv.w_off[lf]; e < tv.w_off[lf + 1]; ++e) {
-            const int c = tv.w_idx[e];
-            for (int d = lane; d < K; d += 32) s_c[wid][d] = mpole[(size_t)c * K + d];
-            __syncwarp();
-            for (int d = lane; d < KH; d += 32) {
-                double g[3];
-                mpole_grad_dof(s_c[wid], d, g);
-                s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
-            }
-            __syncwarp();
-            const double wcx = tv.center[4 * c], wcy = tv.center[4 * c + 1], wcz = tv.center[4 * c + 2];
-            const double winv = 1.0 / (2.0 * tv.center[4 * c + 3]);
-            const double ux = (x - wcx) * winv, uy = (y - wcy) * winv, uz = (z - wcz) * winv;
-            double ax = 0, ay = 0, az = 0, ph = 0;
-            for_singular<P + 1>(ux, uy, uz, [&](int n, int m, double re, double im) {
-                const double w = (m == 0) ? 1.0 : 2.0;
-                const int dr = dof_re(n, m);
-                if (POT && n <= P) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : 0.0));
-                ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : 0.0));
-                ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : 0.0));
-                az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : 0.0));
-            });
-            gx += ax * winv * winv; gy += ay * winv * winv; gz += az * winv * winv;
-            phi += ph * winv;
-            __syncwarp();
-        }
-        if (act) {
-            far[4 * (size_t)i] = gx; far[4 * (size_t)i + 1] = gy; far[4 * (size_t)i + 2] = gz; far[4 * (size_t)i + 3] = phi;
-        }
-    }
-}
-
 // ---- leaf near field (P2P over U) + final combine ----------------------------------------
 template <bool POT>
 __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot) {
@@ -373,10 +235,10 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
     OGX_CUDA(cudaEventRecord(h.ev[2], st));
     // upward
-    const size_t p2x_smem = 4 * 32 * LD * sizeof(double);
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
-    k_p2x<P, 0><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
+    const size_t p2x_smem = p2x_smem_bytes<P, double>();
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    k_p2x<P, 0, double><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
     for (int l = h.max_level - 1; l >= 0; --l) {
         const int first = h.level_off[l], count = h.level_off[l + 1] - first;
         if (count > 0) { k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
@@ -392,7 +254,7 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));
     // P2L
-    k_p2x<P, 1><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
+    k_p2x<P, 1, double><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
     // L2L top-down
     for (int l = 0; l <= h.max_level; ++l) {
@@ -402,8 +264,8 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     // leaves
     const bool pot = d_pot != nullptr;
-    if (pot) { k_leaf_far<P, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
-    else { k_leaf_far<P, false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    if (pot) { k_leaf_far<P, true, double><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    else { k_leaf_far<P, false, double><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
     if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
     else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
@@ -412,7 +274,153 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     return OGX_OK;
 }
 
+// ---- mixed form ---------------------------------------------------------------------
+// host emulation of cvt.rna.tf32.f32 (round to nearest, ties away from zero)
+inline float rna_tf32(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u = (u + 0x1000u) & ~0x1FFFu;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// Operator images for the tensor-core M2L, per offset o, K-chunk c and part (hi, lo):
+// rows = output dofs 1..K-1, K-major in the canonical no-swizzle core-matrix layout,
+// exactly the bytes one pipeline stage holds, so one bulk copy moves a chunk.
+// Also row 0 of every T_o (for the degree-0 local coefficient of potentials).
+template <int P>
+int ensure_mixed_tables(Handle& h) {
+    using C = mixed::TcCfg<P>;
+    if (h.mix_ready_p == P) return OGX_OK;
+    const int K = C::K;
+    std::vector<double> T((size_t)K * K);
+    std::vector<uint8_t> img((size_t)343 * C::NCH * 2 * C::B_BYTES, 0);
+    std::vector<double> row0((size_t)343 * K, 0.0);
+    for (int o = 0; o < 343; ++o) {
+        const int ox = o % 7 - 3, oy = (o / 7) % 7 - 3, oz = o / 49 - 3;
+        if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) <= 1) continue;
+        build_operator(2, P, o, T.data());
+        for (int k = 0; k < K; ++k) row0[(size_t)o * K + k] = T[k];
+        for (int c = 0; c < C::NCH; ++c) {
+            uint8_t* hi = img.data() + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
+            uint8_t* lo = hi + C::B_BYTES;
+            for (int jr = 0; jr < C::N; ++jr)
+                for (int kk = 0; kk < C::CH * 8; ++kk) {
+                    const int k = c * C::CH * 8 + kk;
+                    if (k >= K) continue;
+                    const double x = T[(size_t)(jr + 1) * K + k];
+                    const float vh = rna_tf32((float)x);
+                    const float vl = rna_tf32((float)(x - (double)vh));
+                    const int off = mixed::core_off(jr, kk, C::SBO);
+                    std::memcpy(hi + off, &vh, 4);
+                    std::memcpy(lo + off, &vl, 4);
+                }
+        }
+    }
+    uint8_t* d_img;
+    double* d_row0;
+    OGX_TRY(arena_get(h.ws, S_MIX_TOPS, img.size(), &d_img));
+    OGX_TRY(arena_get(h.ws, S_MIX_ROW0, row0.size(), &d_row0));
+    OGX_CUDA(cudaMemcpy(d_img, img.data(), img.size(), cudaMemcpyHostToDevice));
+    OGX_CUDA(cudaMemcpy(d_row0, row0.data(), row0.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h.d_tc_img = d_img;
+    h.d_tc_row0 = d_row0;
+    h.mix_ready_p = P;
+    return OGX_OK;
+}
+
+template <int P>
+int run_mixed(Handle& h, double* d_acc, double* d_pot) {
+    using C = mixed::TcCfg<P>;
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int LD = K | 1;
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    OGX_TRY(harm_tables_ready(h.device));
+    if constexpr (C::SUPPORTED) OGX_TRY(ensure_mixed_tables<P>(h));
+    double *M, *L, *Lown, *far;
+    float *mhi, *mlo;
+    OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
+    OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
+    OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
+    OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
+    OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
+    OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
+    OGX_CUDA(cudaEventRecord(h.ev[2], st));
+    // upward (FP64)
+    const size_t p2x_smem = p2x_smem_bytes<P, float>();
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    k_p2x<P, 0, float><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
+    for (int l = h.max_level - 1; l >= 0; --l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) { k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+    }
+    {
+        const int64_t tot = (int64_t)tv.nb * C::KPAD;
+        if constexpr (C::SUPPORTED) { mixed::k_split_mpole<P><<<(int)((tot + 255) / 256), 256, 0, st>>>(M, tv.nb, mhi, mlo); ++h.launches; }
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[3], st));
+    // M2L on the tensor cores
+    OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
+    if (h.ntgt > 0) {
+        if constexpr (C::SUPPORTED) {
+            OGX_CUDA(cudaFuncSetAttribute(mixed::k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, mixed::TC_THREADS, C::SMEM, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, mhi,
+                                                                                 mlo, h.d_tc_img, Lown, h.d_err); ++h.launches;
+            if (d_pot) {
+                mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, st>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,
+                                                                             h.d_tc_row0, M, Lown); ++h.launches;
+            }
+        } else {
+            // p > 10: the accumulators of one tile do not fit TMEM; the FP64 M2L serves these orders
+            const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
+            OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
+            k_m2l_fp64<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M,
+                                                                           Lown); ++h.launches;
+        }
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[4], st));
+    k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
+    OGX_CUDA(cudaEventRecord(h.ev[5], st));
+    for (int l = 0; l <= h.max_level; ++l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) { k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+    }
+    OGX_CUDA(cudaEventRecord(h.ev[6], st));
+    const bool pot = d_pot != nullptr;
+    if (pot) { k_leaf_far<P, true, float><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    else { k_leaf_far<P, false, float><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    const double G = h.prm.G;
+    const float eps2 = (float)(h.prm.eps * h.prm.eps);
+    if (pot) { mixed::k_leaf_near32<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
+    else { mixed::k_leaf_near32<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
+    OGX_CUDA(cudaEventRecord(h.ev[7], st));
+    OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
 }  // namespace
+
+int fmm_mixed(Handle& h, double* d_acc, double* d_pot) {
+    switch (h.prm.p) {
+        case 1: return run_mixed<1>(h, d_acc, d_pot);
+        case 2: return run_mixed<2>(h, d_acc, d_pot);
+        case 3: return run_mixed<3>(h, d_acc, d_pot);
+        case 4: return run_mixed<4>(h, d_acc, d_pot);
+        case 5: return run_mixed<5>(h, d_acc, d_pot);
+        case 6: return run_mixed<6>(h, d_acc, d_pot);
+        case 7: return run_mixed<7>(h, d_acc, d_pot);
+        case 8: return run_mixed<8>(h, d_acc, d_pot);
+        case 9: return run_mixed<9>(h, d_acc, d_pot);
+        case 10: return run_mixed<10>(h, d_acc, d_pot);
+        case 11: return run_mixed<11>(h, d_acc, d_pot);
+        case 12: return run_mixed<12>(h, d_acc, d_pot);
+        default: return OGX_ERR_INVALID;
+    }
+}
 
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot) {
     switch (h.prm.p) {

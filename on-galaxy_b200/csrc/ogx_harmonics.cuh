@@ -25,16 +25,57 @@
 
 namespace ogx {
 
+constexpr int kTab = kDegMax + 2;
+
 struct HarmTables {
-    double a[kDegMax + 2];
-    double b[kDegMax + 2];
-    double A[kDegMax + 2][kDegMax + 2];
-    double B[kDegMax + 2][kDegMax + 2];
+    double a[kTab];
+    double b[kTab];
+    double A[kTab][kTab];
+    double B[kTab][kTab];
+    // gradient-coefficient constants (derivative recurrences of FmmExpansions3D.hpp:111-129)
+    double gz[kTab][kTab], gp[kTab][kTab], gm[kTab][kTab];  // local  -> degree n (from degree n+1)
+    double hz[kTab][kTab], hp[kTab][kTab], hm[kTab][kTab];  // mpole  -> degree n (from degree n-1)
 };
+
+// the reference's derivative coefficients (FmmExpansions3D.hpp:111-129)
+inline double ref_cz_R(int n, int m) { return std::sqrt(double(n * n - m * m)); }
+inline double ref_cp_R(int n, int m) { return ((m >= 0) ? -1.0 : 1.0) * std::sqrt(double((n - m) * (n - m - 1))); }
+inline double ref_cm_R(int n, int m) { return ((m > 0) ? 1.0 : -1.0) * std::sqrt(double((n + m) * (n + m - 1))); }
+inline double ref_dz_S(int n, int m) { return -std::sqrt(double((n + 1) * (n + 1) - m * m)); }
+inline double ref_dp_S(int n, int m) { return ((m >= 0) ? -1.0 : 1.0) * std::sqrt(double((n + m + 1) * (n + m + 2))); }
+inline double ref_dm_S(int n, int m) { return ((m > 0) ? 1.0 : -1.0) * std::sqrt(double((n - m + 1) * (n - m + 2))); }
 
 // One copy per translation unit (whole-program compilation, no device linking);
 // every unit that launches harmonic kernels calls harm_tables_ready() first.
 static __constant__ HarmTables c_harm;
+
+static inline void fill_harm_tables(HarmTables& t) {
+    t = HarmTables{};
+    for (int m = 0; m < kTab; ++m) {
+        t.a[m] = m > 0 ? std::sqrt((2.0 * m - 1.0) / (2.0 * m)) : 1.0;
+        t.b[m] = std::sqrt(2.0 * m + 1.0);
+    }
+    for (int n = 0; n < kTab; ++n)
+        for (int m = 0; m < kTab; ++m) {
+            if (n >= m + 2) {
+                const double d = std::sqrt((double)(n * n - m * m));
+                t.A[n][m] = (2.0 * n - 1.0) / d;
+                t.B[n][m] = std::sqrt((double)((n - 1) * (n - 1) - m * m)) / d;
+            }
+            if (m <= n) {
+                // G_n^m from L_{n+1}^{m}, L_{n+1}^{m-1}, L_{n+1}^{m+1}
+                t.gz[n][m] = ref_cz_R(n + 1, m);
+                t.gp[n][m] = ref_cp_R(n + 1, m - 1);
+                t.gm[n][m] = ref_cm_R(n + 1, m + 1);
+                // H_n^m from M_{n-1}^{m}, M_{n-1}^{m-1}, M_{n-1}^{m+1} (zero where the source order is absent)
+                if (n >= 1) {
+                    t.hz[n][m] = (m <= n - 1) ? ref_dz_S(n - 1, m) : 0.0;
+                    t.hp[n][m] = (std::abs(m - 1) <= n - 1) ? ref_dp_S(n - 1, m - 1) : 0.0;
+                    t.hm[n][m] = (m + 1 <= n - 1) ? ref_dm_S(n - 1, m + 1) : 0.0;
+                }
+            }
+        }
+}
 
 static inline int harm_tables_ready(int device) {
     static std::mutex mu;
@@ -42,18 +83,8 @@ static inline int harm_tables_ready(int device) {
     std::lock_guard<std::mutex> lk(mu);
     if (device < 0 || device >= 64) return OGX_ERR_INVALID;
     if (done[device]) return OGX_OK;
-    HarmTables t{};
-    for (int m = 0; m < kDegMax + 2; ++m) {
-        t.a[m] = m > 0 ? std::sqrt((2.0 * m - 1.0) / (2.0 * m)) : 1.0;
-        t.b[m] = std::sqrt(2.0 * m + 1.0);
-    }
-    for (int n = 0; n < kDegMax + 2; ++n)
-        for (int m = 0; m < kDegMax + 2; ++m)
-            if (n >= m + 2) {
-                const double d = std::sqrt((double)(n * n - m * m));
-                t.A[n][m] = (2.0 * n - 1.0) / d;
-                t.B[n][m] = std::sqrt((double)((n - 1) * (n - 1) - m * m)) / d;
-            }
+    HarmTables t;
+    fill_harm_tables(t);
     const cudaError_t e = cudaMemcpyToSymbol(c_harm, &t, sizeof(t));
     if (e != cudaSuccess) {
         set_last_error(OGX_ERR_CUDA, std::string("harmonic tables: ") + cudaGetErrorString(e));
@@ -138,6 +169,13 @@ __device__ __forceinline__ void coef_get(const T* c, int n, int m, T& re, T& im)
     if (m < 0) im = -im;
 }
 
+__device__ __forceinline__ void dof_decode(int d, int& n, int& m, int& part) {
+    n = (int)floorf(sqrtf((float)d) + 1e-4f);
+    const int r = d - n * n;
+    m = (r + 1) >> 1;
+    part = (r == 0) ? 0 : ((r - 1) & 1);
+}
+
 // Gradient coefficients of a local expansion (degree P -> P-1), in the real
 // layout, for the three axes.  From the derivative recurrences of
 // FmmExpansions3D.hpp:111-119 as used by localField (:215-235):
@@ -145,28 +183,20 @@ __device__ __forceinline__ void coef_get(const T* c, int n, int m, T& re, T& im)
 //   Gx_n^m = (cp_R(n+1,m-1) L_{n+1}^{m-1} + cm_R(n+1,m+1) L_{n+1}^{m+1}) / 2
 //   Gy_n^m = -i (cp_R(n+1,m-1) L_{n+1}^{m-1} - cm_R(n+1,m+1) L_{n+1}^{m+1}) / 2
 // Every returned value is for one real dof index `d` of degree <= P-1.
-template <class T>
-__device__ __forceinline__ void local_grad_dof(const T* L, int d, T g[3]) {
-    const int n = (int)floorf(sqrtf((float)d) + 1e-4f);
-    const int r = d - n * n;
-    const int m = (r + 1) >> 1;
-    const int part = (r == 0) ? 0 : ((r - 1) & 1);
+template <class Tin, class T>
+__device__ __forceinline__ void local_grad_dof(const Tin* L, int d, T g[3]) {
+    int n, m, part;
+    dof_decode(d, n, m, part);
     const int N = n + 1;
-    T lr, li, pr, pi, mr, mi;
+    Tin lr, li, pr, pi, mr, mi;
     coef_get(L, N, m, lr, li);
-    coef_get(L, N, m - 1, mr, mi);   // L_{n+1}^{m-1}
-    coef_get(L, N, m + 1, pr, pi);   // L_{n+1}^{m+1}
-    const T czr = sqrt((T)(N * N - m * m));
-    const int mm = m - 1, mp = m + 1;
-    const T cpr = ((mm >= 0) ? -1 : 1) * sqrt((T)((N - mm) * (N - mm - 1)));
-    const T cmr = ((mp > 0) ? 1 : -1) * sqrt((T)((N + mp) * (N + mp - 1)));
-    const T xr = T(0.5) * (cpr * mr + cmr * pr), xi = T(0.5) * (cpr * mi + cmr * pi);
-    // -i/2 (a - b) = (Im(a-b)/2) - i (Re(a-b)/2)
-    const T dr = cpr * mr - cmr * pr, di = cpr * mi - cmr * pi;
-    const T yr = T(0.5) * di, yi = T(-0.5) * dr;
-    const T zr = czr * lr, zi = czr * li;
-    if (part == 0) { g[0] = xr; g[1] = yr; g[2] = zr; }
-    else { g[0] = xi; g[1] = yi; g[2] = zi; }
+    coef_get(L, N, m - 1, mr, mi);
+    coef_get(L, N, m + 1, pr, pi);
+    const double czr = c_harm.gz[n][m], cpr = c_harm.gp[n][m], cmr = c_harm.gm[n][m];
+    const double xr = 0.5 * (cpr * mr + cmr * pr), xi = 0.5 * (cpr * mi + cmr * pi);
+    const double dr = cpr * mr - cmr * pr, di = cpr * mi - cmr * pi;  // -i/2 (a - b)
+    if (part == 0) { g[0] = (T)xr; g[1] = (T)(0.5 * di); g[2] = (T)(czr * lr); }
+    else { g[0] = (T)xi; g[1] = (T)(-0.5 * dr); g[2] = (T)(czr * li); }
 }
 
 // Gradient coefficients of a multipole expansion (degree P -> P+1), from
@@ -174,28 +204,21 @@ __device__ __forceinline__ void local_grad_dof(const T* L, int d, T g[3]) {
 //   Hz_n^m = dz_S(n-1,m) M_{n-1}^m
 //   Hx_n^m = (dp_S(n-1,m-1) M_{n-1}^{m-1} + dm_S(n-1,m+1) M_{n-1}^{m+1}) / 2
 //   Hy_n^m = -i (dp_S(n-1,m-1) M_{n-1}^{m-1} - dm_S(n-1,m+1) M_{n-1}^{m+1}) / 2
-template <class T>
-__device__ __forceinline__ void mpole_grad_dof(const T* M, int d, T g[3]) {
-    const int n = (int)floorf(sqrtf((float)d) + 1e-4f);
-    const int r = d - n * n;
-    const int m = (r + 1) >> 1;
-    const int part = (r == 0) ? 0 : ((r - 1) & 1);
+template <class Tin, class T>
+__device__ __forceinline__ void mpole_grad_dof(const Tin* M, int d, T g[3]) {
+    int n, m, part;
+    dof_decode(d, n, m, part);
     if (n == 0) { g[0] = g[1] = g[2] = 0; return; }
     const int N = n - 1;
-    T lr, li, pr, pi, mr, mi;
+    Tin lr, li, pr, pi, mr, mi;
     coef_get(M, N, m, lr, li);
     coef_get(M, N, m - 1, mr, mi);
     coef_get(M, N, m + 1, pr, pi);
-    const T dzs = -sqrt((T)((N + 1) * (N + 1) - m * m));
-    const int mm = m - 1, mp = m + 1;
-    const T dps = ((mm >= 0) ? -1 : 1) * sqrt((T)((N + mm + 1) * (N + mm + 2)));
-    const T dms = ((mp > 0) ? 1 : -1) * sqrt((T)((N - mp + 1) * (N - mp + 2)));
-    const T xr = T(0.5) * (dps * mr + dms * pr), xi = T(0.5) * (dps * mi + dms * pi);
-    const T dr = dps * mr - dms * pr, di = dps * mi - dms * pi;
-    const T yr = T(0.5) * di, yi = T(-0.5) * dr;
-    const T zr = (m <= N) ? dzs * lr : T(0), zi = (m <= N) ? dzs * li : T(0);
-    if (part == 0) { g[0] = xr; g[1] = yr; g[2] = zr; }
-    else { g[0] = xi; g[1] = yi; g[2] = zi; }
+    const double dzs = c_harm.hz[n][m], dps = c_harm.hp[n][m], dms = c_harm.hm[n][m];
+    const double xr = 0.5 * (dps * mr + dms * pr), xi = 0.5 * (dps * mi + dms * pi);
+    const double dr = dps * mr - dms * pr, di = dps * mi - dms * pi;
+    if (part == 0) { g[0] = (T)xr; g[1] = (T)(0.5 * di); g[2] = (T)(dzs * lr); }
+    else { g[0] = (T)xi; g[1] = (T)(-0.5 * dr); g[2] = (T)(dzs * li); }
 }
 
 }  // namespace ogx

@@ -74,7 +74,7 @@ enum Slot {
     S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, S_TGT_TILE, S_TGT_PKEY, S_TGT_PBOX,
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
-    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN,
+    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR,
     S_NUM_SLOTS
 };
 
@@ -114,6 +114,8 @@ struct DevCounts {
     int64_t p2p_pairs, m2p_evals, p2l_evals;
     int64_t adj_mismatch;
     int64_t v_total;
+    int32_t kernel_error;  // set by kernels whose bounded waits ran out
+    int32_t pad_err;
     int32_t nonleaf_level[kMaxDepth + 2];
 };
 
@@ -166,8 +168,11 @@ struct Handle {
     TreeView tv{};
     bool tree_valid = false;
     // mixed-precision tables
-    float* d_m2l_tf32 = nullptr;
     int mix_ready_p = -1;
+    uint8_t* d_tc_img = nullptr;   // tensor-core M2L operator images (hi/lo)
+    double* d_tc_row0 = nullptr;   // row 0 of every M2L operator
+    int* d_err = nullptr;          // device error word of the bounded waits
+    int* h_err = nullptr;          // pinned copy
     // M2L targets (levels >= 2) sorted by child octant
     int ntgt = 0;
     const uint32_t* tgt_key = nullptr;

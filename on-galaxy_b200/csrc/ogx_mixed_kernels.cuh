@@ -1,0 +1,477 @@
+// ogx_mixed_kernels.cuh -- kernels of the mixed-precision form.
+//
+// M2L on the 5th-generation tensor cores (tcgen05, kind::tf32, TMEM accumulators).
+// The reference applies fmm::M2L pair by pair (src3d/FmmExpansions3D.hpp:273-299,
+// called per V-list entry in src3d/AdaptiveFMM3D.hpp:78-81).  Here:
+//   * a CTA owns 128 targets that share their octant t inside their parents
+//     (any level: the scaled operator is level independent);
+//   * the V list of every such target is the children s of its parent's
+//     colleague slots D with offset o = 2(D-1) + s - t, max|o| >= 2 (189
+//     combinations for a given t); for one combination every target has at
+//     most one source, so the sources of the 128 targets form the rows of a
+//     dense operand A (128 x K, zero rows where absent) and the translation is
+//     D[128 x N] = A . T_o^T with one operator matrix T_o for the whole tile;
+//   * split precision: multipoles and operators are split into TF32 hi + lo
+//     parts and D accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32
+//     (the dropped lo x lo term is ~2^-22 relative);
+//   * accumulation: FP32 accumulation over all ~6000 MMA steps of a tile loses
+//     ~1e-5 of the (strongly cancelling) far field, so every combination gets a
+//     fresh FP32 accumulator (two ping-pong buffers in TMEM) that the epilogue
+//     warps drain into an FP64 accumulator also kept in TMEM (two 32-bit
+//     columns per value) while the MMA warp proceeds with the next combination;
+//   * operands: A rows are gathered with cp.async into the canonical K-major
+//     no-swizzle layout (8-row x 16-byte core matrices); each T_o chunk is a
+//     pre-laid-out image copied by the TMA bulk engine (cp.async.bulk, no
+//     multicast); K is cut into chunks of 32 so 4 stages pipeline through
+//     mbarriers; one warp issues the MMAs (one lane), four warps produce the
+//     operands, drain the accumulators and write the result.
+// Output degree 0 (L_0^0, only needed for potentials) is excluded from N.
+// TMEM holds 2 x N FP32 + 2 x N FP64-halves columns, so the tensor-core path
+// serves p <= 10 (N <= 128); higher orders use the FP64 M2L kernel.
+//
+// Near field in FP32 on leaf-centred double-float coordinates (hi + lo FP32
+// relative to the target leaf centre, shift in FP64), r^-1 from rsqrt plus one
+// Newton step, every U-list entry's partial sum folded into a compensated
+// (Kahan) accumulator.
+#pragma once
+
+#include "ogx_harmonics.cuh"
+#include "ogx_sm100.cuh"
+
+namespace ogx {
+namespace mixed {
+
+template <int P>
+struct TcCfg {
+    static constexpr int K = (P + 1) * (P + 1);
+    static constexpr int KPAD = (K + 7) / 8 * 8;
+    static constexpr int NKS = KPAD / 8;      // K-steps of the MMA (8 tf32 each)
+    static constexpr int CH = 4;              // K-steps per pipeline chunk
+    static constexpr int NCH = (NKS + CH - 1) / CH;
+    static constexpr int N = K - 1;           // output dofs 1..K-1
+    static constexpr int NPAD = (N + 15) / 16 * 16;
+    static constexpr int M = 128;
+    static constexpr int SBO = CH * 2 * 128;  // bytes between 8-row groups
+    static constexpr int A_BYTES = (M / 8) * SBO;
+    static constexpr int B_BYTES = (NPAD / 8) * SBO;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int STAGES = (220 * 1024 / STAGE_BYTES) >= 4 ? 4 : (220 * 1024 / STAGE_BYTES);
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024;
+    static constexpr int ACC64 = 2 * NPAD;    // first column of the FP64 accumulator
+    static constexpr int TMEM_COLS = 512;
+    static constexpr bool SUPPORTED = 4 * NPAD <= 512 && STAGES >= 2;
+};
+
+// byte offset of element (row, kk) inside one operand stage (kk < CH*8)
+__host__ __device__ __forceinline__ int core_off(int row, int kk, int sbo) {
+    return (row >> 3) * sbo + (kk >> 2) * 128 + (row & 7) * 16 + (kk & 3) * 4;
+}
+
+constexpr int TC_THREADS = 160;  // warps 0-3 producers + epilogue, warp 4 MMA issuer
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Add the FP32 combination result in D buffer `a` to the FP64 accumulator (this
+// warp's 32 lanes); `first` initialises the accumulator instead of adding.
+template <int NPAD, int ACC64>
+__device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first) {
+#pragma unroll 1
+    for (int c16 = 0; c16 < NPAD / 16; ++c16) {
+        uint32_t v[16], lo[16], hi[16];
+        sm100::tmem_ld16(tmem_lane + a * NPAD + c16 * 16, v);
+        if (!first) {
+            sm100::tmem_ld16(tmem_lane + ACC64 + c16 * 32, lo);
+            sm100::tmem_ld16(tmem_lane + ACC64 + c16 * 32 + 16, hi);
+        }
+        sm100::tmem_ld_wait();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            double s = (double)__uint_as_float(v[k]);
+            if (!first) s += __hiloint2double((int)hi[k], (int)lo[k]);
+            lo[k] = (uint32_t)__double2loint(s);
+            hi[k] = (uint32_t)__double2hiint(s);
+        }
+        tmem_st16(tmem_lane + ACC64 + c16 * 32, lo);
+        tmem_st16(tmem_lane + ACC64 + c16 * 32 + 16, hi);
+    }
+    tmem_st_wait();
+}
+
+template <int P>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_m2l_tc(TreeView tv, const uint32_t* __restrict__ tgt_key, const uint32_t* __restrict__ tgt_box,
+             const float* __restrict__ mhi, const float* __restrict__ mlo, const uint8_t* __restrict__ btab,
+             double* __restrict__ lown, int* err) {
+    using C = TcCfg<P>;
+    static_assert(C::SUPPORTED, "tensor-core M2L serves p <= 10");
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ uint64_t afull[C::STAGES], bfull[C::STAGES], empty[C::STAGES], dfull[2], dempty[2], fin;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    __shared__ int s_t;
+    __shared__ int s_parent[128];
+    __shared__ uint32_t s_mask[6];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int base = blockIdx.x * 128;
+    if (tid == 0) {
+        s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
+        s_abort = 0;
+        for (int s = 0; s < C::STAGES; ++s) {
+            sm100::mbar_init(&afull[s], 128);
+            sm100::mbar_init(&bfull[s], 1);
+            sm100::mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            sm100::mbar_init(&dfull[a], 1);
+            sm100::mbar_init(&dempty[a], 128);
+        }
+        sm100::mbar_init(&fin, 1);
+        sm100::fence_mbar_init();
+    }
+    if (tid < 6) s_mask[tid] = 0;
+    __syncthreads();
+    const int t = s_t;
+    if (t < 0) return;
+    const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
+    if (warp == 4) sm100::tmem_alloc(&s_tmem, C::TMEM_COLS);
+    int myb = -1;
+    if (tid < 128) {
+        const uint32_t key = tgt_key[base + tid];
+        myb = (key == (uint32_t)t) ? (int)tgt_box[base + tid] : -1;
+        s_parent[tid] = (myb >= 0) ? tv.parent[myb] : -1;
+    }
+    __syncthreads();
+    // presence mask over the 189 (D, s) combinations of octant t
+    if (tid < 128) {
+        const int par = s_parent[tid];
+        int ci = 0;
+        for (int D = 0; D < 27; ++D) {
+            const int Q = (par >= 0) ? tv.col[27 * par + D] : -1;
+            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+            for (int s = 0; s < 8; ++s) {
+                const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
+                const bool has = (Q >= 0) && (tv.child[8 * Q + s] >= 0);
+                const unsigned bal = __ballot_sync(0xffffffffu, has);
+                if (lane == 0 && bal) atomicOr(&s_mask[ci >> 5], 1u << (ci & 31));
+                ++ci;
+            }
+        }
+    }
+    sm100::tc_fence_before();
+    __syncthreads();
+    sm100::tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (warp == 4) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            constexpr uint32_t idesc = sm100::idesc_tf32(C::M, C::NPAD);
+            int u = 0, cc = 0;
+            for (int ci = 0; ci < 189 && !s_abort; ++ci) {
+                if (!((s_mask[ci >> 5] >> (ci & 31)) & 1u)) continue;
+                const int a = cc & 1;
+                if (cc >= 2) {
+                    if (!sm100::mbar_wait(&dempty[a], ((cc >> 1) - 1) & 1, &s_abort)) {
+                        s_abort = 1;
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    sm100::tc_fence_after();
+                }
+                const uint32_t dcol = tmem + a * C::NPAD;
+                uint32_t accum = 0;
+                for (int c = 0; c < C::NCH && !s_abort; ++c, ++u) {
+                    const int s = u % C::STAGES;
+                    const uint32_t ph = (u / C::STAGES) & 1;
+                    if (!sm100::mbar_wait(&afull[s], ph, &s_abort) || !sm100::mbar_wait(&bfull[s], ph, &s_abort)) {
+                        s_abort = 1;
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    sm100::tc_fence_after();
+                    const uint32_t st = sm100::smem_u32(smem + (size_t)s * C::STAGE_BYTES);
+                    const uint32_t a_hi = st, a_lo = st + C::A_BYTES, b_hi = st + 2 * C::A_BYTES,
+                                   b_lo = b_hi + C::B_BYTES;
+                    const int nks = min(C::CH, C::NKS - c * C::CH);
+                    for (int ks = 0; ks < nks; ++ks) {
+                        const uint32_t ko = ks * 256;
+                        sm100::mma_tf32(dcol, sm100::smem_desc(a_hi + ko, 128, C::SBO), sm100::smem_desc(b_hi + ko, 128, C::SBO),
+                                        idesc, accum);
+                        accum = 1;
+                        sm100::mma_tf32(dcol, sm100::smem_desc(a_hi + ko, 128, C::SBO), sm100::smem_desc(b_lo + ko, 128, C::SBO),
+                                        idesc, 1);
+                        sm100::mma_tf32(dcol, sm100::smem_desc(a_lo + ko, 128, C::SBO), sm100::smem_desc(b_hi + ko, 128, C::SBO),
+                                        idesc, 1);
+                    }
+                    sm100::mma_commit(&empty[s]);
+                }
+                sm100::mma_commit(&dfull[a]);
+                ++cc;
+            }
+            // completion of every MMA this thread issued (normal end and abort alike)
+            sm100::mma_commit(&fin);
+            if (!sm100::mbar_wait(&fin, 0, nullptr)) atomicExch(err, 1);
+        }
+        __syncwarp();
+    } else {
+        // ---------------- producers (thread tid owns target row tid) ----------------
+        const int r = tid;
+        const int par = s_parent[r];
+        const uint32_t tmem_lane = tmem + ((uint32_t)(warp * 32) << 16);
+        int u = 0, cc = 0, ci = 0;
+        bool bulk_pending[C::STAGES];
+        uint32_t bulk_phase[C::STAGES];
+        for (int s = 0; s < C::STAGES; ++s) bulk_pending[s] = false, bulk_phase[s] = 0;
+        auto drain = [&](int which) -> bool {
+            const int a = which & 1;
+            if (!sm100::mbar_wait(&dfull[a], (which >> 1) & 1, &s_abort)) {
+                s_abort = 1;
+                atomicExch(err, 1);
+                return false;
+            }
+            sm100::tc_fence_after();
+            drain_combo<C::NPAD, C::ACC64>(tmem_lane, a, which == 0);
+            sm100::tc_fence_before();
+            sm100::mbar_arrive(&dempty[a]);
+            return true;
+        };
+        for (int D = 0; D < 27 && !s_abort; ++D) {
+            const int Q = (par >= 0) ? tv.col[27 * par + D] : -1;
+            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+            for (int s8 = 0; s8 < 8 && !s_abort; ++s8) {
+                const int ox = 2 * Dx + (s8 & 1) - tx, oy = 2 * Dy + ((s8 >> 1) & 1) - ty, oz = 2 * Dz + ((s8 >> 2) & 1) - tz;
+                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
+                const int my_ci = ci++;
+                if (!((s_mask[my_ci >> 5] >> (my_ci & 31)) & 1u)) continue;
+                const int src = (Q >= 0) ? tv.child[8 * Q + s8] : -1;
+                const int o = (ox + 3) + 7 * (oy + 3) + 49 * (oz + 3);
+                for (int c = 0; c < C::NCH; ++c, ++u) {
+                    const int s = u % C::STAGES;
+                    if (u >= C::STAGES) {
+                        if (!sm100::mbar_wait(&empty[s], ((u / C::STAGES) - 1) & 1, &s_abort)) {
+                            s_abort = 1;
+                            atomicExch(err, 1);
+                            break;
+                        }
+                        bulk_pending[s] = false;
+                    }
+                    uint8_t* st = smem + (size_t)s * C::STAGE_BYTES;
+                    if (r == 0) {
+                        const uint8_t* bsrc = btab + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
+                        sm100::mbar_arrive_expect_tx(&bfull[s], 2 * C::B_BYTES);
+                        sm100::bulk_g2s(st + 2 * C::A_BYTES, bsrc, C::B_BYTES, &bfull[s]);
+                        sm100::bulk_g2s(st + 2 * C::A_BYTES + C::B_BYTES, bsrc + C::B_BYTES, C::B_BYTES, &bfull[s]);
+                        bulk_pending[s] = true;
+                        bulk_phase[s] = (u / C::STAGES) & 1;
+                    }
+                    const int k0 = c * C::CH * 8;
+                    const int nq = min(2 * C::CH, (C::KPAD - k0) / 4);
+                    if (src >= 0) {
+                        const float* gh = mhi + (size_t)src * C::KPAD + k0;
+                        const float* gl = mlo + (size_t)src * C::KPAD + k0;
+                        for (int q = 0; q < nq; ++q) {
+                            sm100::cp_async16(st + core_off(r, 4 * q, C::SBO), gh + 4 * q);
+                            sm100::cp_async16(st + C::A_BYTES + core_off(r, 4 * q, C::SBO), gl + 4 * q);
+                        }
+                    } else {
+                        for (int q = 0; q < nq; ++q) {
+                            *(float4*)(st + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
+                            *(float4*)(st + C::A_BYTES + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+                    }
+                    sm100::cp_async_commit();
+                    if (u >= 1) {
+                        sm100::cp_async_wait<1>();
+                        sm100::fence_proxy_async();
+                        sm100::mbar_arrive(&afull[(u - 1) % C::STAGES]);
+                    }
+                }
+                // every unit of combination cc is issued: fold combination cc-1 into FP64
+                if (cc >= 1 && !s_abort) drain(cc - 1);
+                ++cc;
+            }
+        }
+        sm100::cp_async_wait<0>();
+        sm100::fence_proxy_async();
+        if (u >= 1 && !s_abort) sm100::mbar_arrive(&afull[(u - 1) % C::STAGES]);
+        if (cc >= 1 && !s_abort) drain(cc - 1);
+        if (s_abort && r == 0) {
+            // let this thread's bulk copies land before the CTA exits
+            for (int s = 0; s < C::STAGES; ++s)
+                if (bulk_pending[s]) sm100::mbar_wait(&bfull[s], bulk_phase[s], nullptr);
+        }
+        // ---------------- epilogue: FP64 accumulator -> L_own (row tid = target) ----------------
+        if (cc >= 1 && !s_abort) {
+            sm100::tc_fence_after();
+            const double inv = (myb >= 0) ? 1.0 / (2.0 * tv.center[4 * myb + 3]) : 0.0;
+#pragma unroll 1
+            for (int c16 = 0; c16 < C::NPAD / 16; ++c16) {
+                uint32_t lo[16], hi[16];
+                sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32, lo);
+                sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32 + 16, hi);
+                sm100::tmem_ld_wait();
+                if (myb >= 0) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int dof = 1 + c16 * 16 + k;
+                        if (dof < C::K)
+                            lown[(size_t)myb * C::K + dof] += __hiloint2double((int)hi[k], (int)lo[k]) * inv;
+                    }
+                }
+            }
+        }
+    }
+    sm100::tc_fence_before();
+    __syncthreads();
+    if (warp == 4) {
+        // the MMA lane waited on `fin` above, so no MMA still writes TMEM here
+        sm100::tc_fence_after();
+        sm100::tmem_dealloc(tmem, C::TMEM_COLS);
+    }
+}
+
+// FP64 multipoles -> TF32 hi/lo pairs, rows padded to KPAD with zeros
+template <int P>
+__global__ void k_split_mpole(const double* __restrict__ M, int nb, float* __restrict__ hi, float* __restrict__ lo) {
+    using C = TcCfg<P>;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nb * C::KPAD) return;
+    const int64_t b = i / C::KPAD;
+    const int k = (int)(i - b * C::KPAD);
+    const double x = (k < C::K) ? M[b * C::K + k] : 0.0;
+    const float h = sm100::to_tf32((float)x);
+    hi[i] = h;
+    lo[i] = sm100::to_tf32((float)(x - (double)h));
+}
+
+// L_0^0 of the M2L (needed only for potentials): FP64 row 0 of every T_o
+template <int P>
+__global__ void __launch_bounds__(128) k_m2l_dof0(TreeView tv, int ntgt_pad, const uint32_t* tgt_key, const uint32_t* tgt_box,
+                                                  const double* row0 /* 343 x K */, const double* M, double* lown) {
+    constexpr int K = (P + 1) * (P + 1);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntgt_pad || tgt_key[i] == 0xFFFFFFFFu) return;
+    const int b = (int)tgt_box[i], t = (int)tgt_key[i];
+    const int par = tv.parent[b];
+    const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
+    double acc = 0.0;
+    for (int D = 0; D < 27; ++D) {
+        const int Q = tv.col[27 * par + D];
+        if (Q < 0) continue;
+        const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+        for (int s = 0; s < 8; ++s) {
+            const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+            if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
+            const int c = tv.child[8 * Q + s];
+            if (c < 0) continue;
+            const double* r0 = row0 + (size_t)((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) * K;
+            for (int k = 0; k < K; ++k) acc = fma(r0[k], M[(size_t)c * K + k], acc);
+        }
+    }
+    lown[(size_t)b * K] += acc / (2.0 * tv.center[4 * b + 3]);
+}
+
+// ---- FP32 near field ------------------------------------------------------------
+// Leaf-centred double-float positions: every coordinate relative to the target
+// leaf centre is held as hi + lo FP32 (hi = fp32(x - c), lo = fp32((x - c) - hi),
+// the shift taken in FP64), so d = (s_hi - t_hi) + (s_lo - t_lo) carries the
+// FP32 relative accuracy of |d| itself even for very close pairs.  Sources of each
+// U-list entry are staged (re-centred) in shared memory once per target leaf.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+constexpr int NEAR_STAGE = 64;
+
+template <bool SELF, bool POT>
+__device__ __forceinline__ void p2p_block(const float4* __restrict__ shi, const float4* __restrict__ slo, int n, int self_q,
+                                          float thx, float thy, float thz, float tlx, float tly, float tlz, float eps2,
+                                          float& ax, float& ay, float& az, float& ph) {
+#pragma unroll 4
+    for (int q = 0; q < n; ++q) {
+        const float4 h = shi[q];
+        const float4 l = slo[q];
+        const float dx = (h.x - thx) + (l.x - tlx);
+        const float dy = (h.y - thy) + (l.y - tly);
+        const float dz = (h.z - thz) + (l.z - tlz);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        const bool self = SELF && (q == self_q);
+        const float r2s = self ? 1.0f : r2;
+        float y = rsqrtf(r2s);
+        y = y * fmaf(-0.5f * r2s, y * y, 1.5f);  // one Newton step
+        const float m = self ? 0.0f : h.w;
+        const float my = m * y;
+        const float w = my * y * y;
+        ax = fmaf(w, dx, ax);
+        ay = fmaf(w, dy, ay);
+        az = fmaf(w, dz, az);
+        if (POT) ph += my;
+    }
+}
+
+template <bool POT>
+__global__ void __launch_bounds__(128) k_leaf_near32(TreeView tv, double G, float eps2, const double* __restrict__ far,
+                                                     double* __restrict__ acc, double* __restrict__ pot) {
+    __shared__ float4 s_hi[4][NEAR_STAGE], s_lo[4][NEAR_STAGE];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= tv.nleaf) return;
+    const int b = tv.leafbox[lf];
+    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+    const double bcx = tv.center[4 * b], bcy = tv.center[4 * b + 1], bcz = tv.center[4 * b + 2];
+    const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int jj = j0 + lane;
+        const bool act = jj < cnt;
+        const int i = f0 + (act ? jj : 0);
+        const double ddx = tv.px[i] - bcx, ddy = tv.py[i] - bcy, ddz = tv.pz[i] - bcz;
+        const float thx = (float)ddx, thy = (float)ddy, thz = (float)ddz;
+        const float tlx = (float)(ddx - (double)thx), tly = (float)(ddy - (double)thy), tlz = (float)(ddz - (double)thz);
+        float sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
+        for (int64_t e = u0; e < u1; ++e) {
+            const int c = tv.u_idx[e];
+            const int s0 = tv.pfirst[c], sc = tv.pcount[c];
+            float ax = 0, ay = 0, az = 0, ph = 0;
+            for (int k0 = 0; k0 < sc; k0 += NEAR_STAGE) {
+                const int n = min(NEAR_STAGE, sc - k0);
+                __syncwarp();
+                for (int q = lane; q < n; q += 32) {
+                    const int j = s0 + k0 + q;
+                    const double ex = tv.px[j] - bcx, ey = tv.py[j] - bcy, ez = tv.pz[j] - bcz;
+                    const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
+                    s_hi[wid][q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
+                    s_lo[wid][q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+                }
+                __syncwarp();
+                if (c == b)
+                    p2p_block<true, POT>(s_hi[wid], s_lo[wid], n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+                else
+                    p2p_block<false, POT>(s_hi[wid], s_lo[wid], n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+            }
+            kahan_add(sx, cx, ax); kahan_add(sy, cy, ay); kahan_add(sz, cz, az);
+            if (POT) kahan_add(sp, cp, ph);
+        }
+        if (act) {
+            const int o = tv.perm[i];
+            acc[3 * (size_t)o] = G * (far[4 * (size_t)i] + ((double)sx - (double)cx));
+            acc[3 * (size_t)o + 1] = G * (far[4 * (size_t)i + 1] + ((double)sy - (double)cy));
+            acc[3 * (size_t)o + 2] = G * (far[4 * (size_t)i + 2] + ((double)sz - (double)cz));
+            if (POT) pot[o] = -G * (far[4 * (size_t)i + 3] + ((double)sp - (double)cp));
+        }
+    }
+}
+
+}  // namespace mixed
+}  // namespace ogx

@@ -484,6 +484,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     RootInfo* root;
     double* part;
     OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    h.d_err = &dc->kernel_error;
     OGX_TRY(arena_get(h.ws, S_ROOT, 1, &root));
     const int nparts = 296;
     OGX_TRY(arena_get(h.ws, S_BBOX, 6 * nparts, &part));
@@ -648,7 +649,7 @@ int lists_build(Handle& h) {
         OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 3, &tk_s, &tb_s));
         h.tgt_key = tk_s;
         h.tgt_box = tb_s;
-        const int tile = 64;
+        const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
         const int npad = ((ntgt + tile - 1) / tile + 8) * tile;
         int* gs;
         uint32_t *pk, *pb;

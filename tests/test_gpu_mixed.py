@@ -1,0 +1,66 @@
+"""GPU checks of the mixed-precision form (FP32 P2P, split-TF32 tensor-core M2L,
+FP64 translations), through the C ABI.
+
+Tolerances (stated per the precision design):
+  * vs the FP64 form at the same p and leaf capacity: RMS <= 5e-6, max_rel <= 1e-3.
+    The budget is set by the FP32 near field: leaf-centred FP32 positions carry an
+    absolute error of 2^-24 x leaf size, so a pair at separation r gets a relative
+    force error ~3e-8 x leaf/r (measured on CPU for Plummer N=2000: RMS 2.6e-6);
+    the 3xTF32 M2L contributes ~2^-22 per product;
+  * vs the FP64 direct oracle: RMS within 5e-6 of the FP64 form's own truncation error.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("p", [2, 4, 6, 8, 10, 12])
+def test_mixed_vs_fp64_form(ogx, golden, p):
+    d = golden("plummer2000_s2")
+    with ogx.AdaptiveFMM3D(p=p, threshold=64, precision=ogx.PREC_FP64) as s64:
+        a64 = s64.compute_accelerations(d["pos"], d["mass"])
+    with ogx.AdaptiveFMM3D(p=p, threshold=64, precision=ogx.PREC_MIXED) as sm:
+        am = sm.compute_accelerations(d["pos"], d["mass"])
+    mx, rms = rel_err(a64, am)
+    assert rms <= 5e-6 and mx <= 1e-3, (p, mx, rms)
+
+
+@pytest.mark.parametrize("name,thr", [("disk4000", 32), ("cube1000_s1", 16), ("clump", 16)])
+def test_mixed_other_inputs(ogx, golden, name, thr):
+    d = golden(name)
+    with ogx.AdaptiveFMM3D(p=8, threshold=thr, precision=ogx.PREC_FP64) as s64:
+        a64 = s64.compute_accelerations(d["pos"], d["mass"])
+    with ogx.AdaptiveFMM3D(p=8, threshold=thr, precision=ogx.PREC_MIXED) as sm:
+        am = sm.compute_accelerations(d["pos"], d["mass"])
+    mx, rms = rel_err(a64, am)
+    assert rms <= 5e-6, (name, mx, rms)
+
+
+def test_mixed_cfg1_vs_direct_and_potentials(ogx, golden, oracle):
+    d = golden("cfg1_plummer16384")
+    with ogx.AdaptiveFMM3D(p=8, threshold=64, precision=ogx.PREC_MIXED) as sm:
+        am, pm = sm.compute_accelerations(d["pos"], d["mass"], with_potential=True)
+    _, rms_m = rel_err(d["direct"], am)
+    _, rms_f = rel_err(d["direct"], d["fmm_p8_t64"])
+    assert abs(rms_m - rms_f) <= 5e-6, (rms_m, rms_f)
+    mx, rms = rel_err(d["fmm_p8_t64"], am)
+    assert rms <= 5e-6, (mx, rms)
+    _, pot_o = oracle.adaptive_fmm(d["pos"], d["mass"], p=8, thr=64)
+    assert np.sqrt(np.sum((pm - pot_o) ** 2) / np.sum(pot_o ** 2)) <= 1e-6
+
+
+def test_mixed_leapfrog_runs_and_tracks_fp64(ogx, golden):
+    d = golden("plummer2000_s2")
+    rng = np.random.default_rng(1)
+    vel = 0.1 * rng.standard_normal(d["pos"].shape)
+    out = []
+    for prec in (ogx.PREC_FP64, ogx.PREC_MIXED):
+        with ogx.AdaptiveFMM3D(p=8, threshold=64, precision=prec) as s:
+            s.upload(d["pos"], vel, d["mass"])
+            s.step(0.01, 5)
+            out.append(s.download())
+    np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-9)
+    assert rel_err(out[0][2], out[1][2])[1] <= 5e-6
