@@ -228,9 +228,11 @@ def main():
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             flush.zero_()
+            torch.cuda.nvtx.range_push("ogx_step")
             starts[k].record(stream)
             solver.step(DT, 1)
             ends[k].record(stream)
+            torch.cuda.nvtx.range_pop()
             phase.append(solver.stats())
         barrier()
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])

@@ -488,6 +488,9 @@ int ogx_tree_boxes(void* handle, int32_t* boxes, double* centers, int32_t* perm)
     OGX_CUDA(cudaMemcpy(leafid.data(), tv.leafid, nb * sizeof(int), cudaMemcpyDeviceToHost));
     OGX_CUDA(cudaMemcpy(pfirst.data(), tv.pfirst, nb * sizeof(int), cudaMemcpyDeviceToHost));
     OGX_CUDA(cudaMemcpy(pcount.data(), tv.pcount, nb * sizeof(int), cudaMemcpyDeviceToHost));
+    // non-leaf occupancy = sum over children (boxes are level-major: children follow parents)
+    for (size_t b = nb; b-- > 1;)
+        if (parent[b] >= 0) pcount[parent[b]] += pcount[b];
     for (size_t b = 0; b < nb; ++b) {
         int32_t* r = boxes + 8 * b;
         r[0] = level[b]; r[1] = coord[3 * b]; r[2] = coord[3 * b + 1]; r[3] = coord[3 * b + 2];

@@ -82,22 +82,71 @@ constexpr size_t p2x_smem_bytes() {
     return (size_t)4 * 32 * ((P + 1) * (P + 1) | 1) * sizeof(T);
 }
 
+// ---- evaluation coefficient sets ---------------------------------------------------
+// Per box (MODE 0): multipole gradient set H (3 x (P+2)^2, degree P+1) and the
+// multipole itself (K), for every box that is a member of some W list (X list
+// non-empty).  Per leaf (MODE 1): local gradient set G (3 x P^2, degree P-1) and
+// the local itself.  Stored in T, one contiguous record per box / leaf:
+//   record = [x-set | y-set | z-set | coefficients]
+template <int P>
+struct EvalLayout {
+    static constexpr int K = (P + 1) * (P + 1);
+    static constexpr int KG = P * P;
+    static constexpr int KH = (P + 2) * (P + 2);
+    static constexpr int HREC = 3 * KH + K;
+    static constexpr int GREC = 3 * KG + K;
+};
+
+template <int P, int MODE, class T>
+__global__ void __launch_bounds__(128) k_eval_coeffs(TreeView tv, int count, const double* __restrict__ coef, T* __restrict__ rec) {
+    using Lo = EvalLayout<P>;
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (k >= count) return;
+    const int b = (MODE == 0) ? k : tv.leafbox[k];
+    if (MODE == 0 && tv.x_off[b] == tv.x_off[b + 1]) return;
+    const double* c = coef + (size_t)b * Lo::K;
+    if (MODE == 0) {
+        T* o = rec + (size_t)k * Lo::HREC;
+        for (int d = lane; d < Lo::KH; d += 32) {
+            T g[3];
+            mpole_grad_dof(c, d, g);
+            o[d] = g[0]; o[Lo::KH + d] = g[1]; o[2 * Lo::KH + d] = g[2];
+        }
+        for (int d = lane; d < Lo::K; d += 32) o[3 * Lo::KH + d] = (T)c[d];
+    } else {
+        T* o = rec + (size_t)k * Lo::GREC;
+        for (int d = lane; d < Lo::KG; d += 32) {
+            T g[3];
+            local_grad_dof(c, d, g);
+            o[d] = g[0]; o[Lo::KG + d] = g[1]; o[2 * Lo::KG + d] = g[2];
+        }
+        for (int d = lane; d < Lo::K; d += 32) o[3 * Lo::KG + d] = (T)c[d];
+    }
+}
+
+// sum over (n, m>=0) of w_m Re(c_nm z_nm) for one dof visit
+template <class T>
+__device__ __forceinline__ T re_term(const T* c, int dr, int m, T re, T im) {
+    return m == 0 ? c[dr] * re : T(2) * (c[dr] * re - c[dr + 1] * im);
+}
+
 // ---- leaf far field: L2P + W-list M2P -----------------------------------------------
 // Warp per leaf, lanes over its bodies.  L2P (fmm::localField, :215-235) and M2P
 // (fmm::multipoleField, :180-200) are evaluated as sum_nm Re(G_nm R_nm(u)) and
-// sum_nm Re(H_nm S_nm(u)) with the gradient coefficient sets G (degree P-1) and
-// H (degree P+1) formed once per (leaf, box) in shared memory; the harmonics are
-// generated column by column so no body holds more than one column.
+// sum_nm Re(H_nm S_nm(u)) with the precomputed coefficient records staged in
+// shared memory once per (leaf, box); the harmonics are generated column by
+// column so no body holds more than one column.
 template <int P, bool POT, class T>
-__global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const double* mpole, const double* local, double* far) {
-    constexpr int K = (P + 1) * (P + 1);
-    constexpr int KG = P * P;
-    constexpr int KH = (P + 2) * (P + 2);
-    __shared__ T s_c[4][K];
-    __shared__ T s_g[4][3][KH];
+__global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const T* __restrict__ hrec, const T* __restrict__ grec,
+                                                  double* __restrict__ far) {
+    using Lo = EvalLayout<P>;
+    constexpr int K = Lo::K, KG = Lo::KG, KH = Lo::KH;
+    __shared__ T s_rec[4][Lo::HREC > Lo::GREC ? Lo::HREC : Lo::GREC];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * 4 + wid;
     if (lf >= tv.nleaf) return;
+    T* sr = s_rec[wid];
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
@@ -110,23 +159,18 @@ __global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const double* mpo
         const double x = tv.px[i], y = tv.py[i], z = tv.pz[i];
         double gx, gy, gz, phi = 0.0;
         {
-            for (int d = lane; d < K; d += 32) s_c[wid][d] = (T)local[(size_t)b * K + d];
-            for (int d = lane; d < KG; d += 32) {
-                T g[3];
-                local_grad_dof(local + (size_t)b * K, d, g);
-                s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
-            }
+            const T* g = grec + (size_t)lf * Lo::GREC;
+            for (int d = lane; d < (POT ? Lo::GREC : 3 * KG); d += 32) sr[d] = g[d];
             __syncwarp();
             const T ux = (T)((x - cx) * inv), uy = (T)((y - cy) * inv), uz = (T)((z - cz) * inv);
             T ax = 0, ay = 0, az = 0, ph = 0;
             for_regular<P>(ux, uy, uz, [&](int n, int m, T re, T im) {
-                const T w = (m == 0) ? T(1) : T(2);
                 const int dr = dof_re(n, m);
-                if (POT) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : T(0)));
+                if (POT) ph += re_term(sr + 3 * KG, dr, m, re, im);
                 if (n < P) {
-                    ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : T(0)));
-                    ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : T(0)));
-                    az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : T(0)));
+                    ax += re_term(sr, dr, m, re, im);
+                    ay += re_term(sr + KG, dr, m, re, im);
+                    az += re_term(sr + 2 * KG, dr, m, re, im);
                 }
             });
             gx = (double)ax * inv; gy = (double)ay * inv; gz = (double)az * inv;
@@ -135,25 +179,19 @@ __global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const double* mpo
         }
         for (int64_t e = w0; e < w1; ++e) {
             const int c = tv.w_idx[e];
-            if (POT)
-                for (int d = lane; d < K; d += 32) s_c[wid][d] = (T)mpole[(size_t)c * K + d];
-            for (int d = lane; d < KH; d += 32) {
-                T g[3];
-                mpole_grad_dof(mpole + (size_t)c * K, d, g);
-                s_g[wid][0][d] = g[0]; s_g[wid][1][d] = g[1]; s_g[wid][2][d] = g[2];
-            }
+            const T* h = hrec + (size_t)c * Lo::HREC;
+            for (int d = lane; d < (POT ? Lo::HREC : 3 * KH); d += 32) sr[d] = h[d];
             __syncwarp();
             const double winv = 1.0 / (2.0 * tv.center[4 * c + 3]);
             const T ux = (T)((x - tv.center[4 * c]) * winv), uy = (T)((y - tv.center[4 * c + 1]) * winv),
                     uz = (T)((z - tv.center[4 * c + 2]) * winv);
             T ax = 0, ay = 0, az = 0, ph = 0;
             for_singular<P + 1>(ux, uy, uz, [&](int n, int m, T re, T im) {
-                const T w = (m == 0) ? T(1) : T(2);
                 const int dr = dof_re(n, m);
-                if (POT && n <= P) ph += w * (s_c[wid][dr] * re - (m ? s_c[wid][dr + 1] * im : T(0)));
-                ax += w * (s_g[wid][0][dr] * re - (m ? s_g[wid][0][dr + 1] * im : T(0)));
-                ay += w * (s_g[wid][1][dr] * re - (m ? s_g[wid][1][dr + 1] * im : T(0)));
-                az += w * (s_g[wid][2][dr] * re - (m ? s_g[wid][2][dr + 1] * im : T(0)));
+                if (POT && n <= P) ph += re_term(sr + 3 * KH, dr, m, re, im);
+                ax += re_term(sr, dr, m, re, im);
+                ay += re_term(sr + KH, dr, m, re, im);
+                az += re_term(sr + 2 * KH, dr, m, re, im);
             });
             gx += (double)ax * winv * winv; gy += (double)ay * winv * winv; gz += (double)az * winv * winv;
             if (POT) phi += (double)ph * winv;

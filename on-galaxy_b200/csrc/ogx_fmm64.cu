@@ -32,68 +32,158 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
-// ---- M2M (MODE 0) / L2L (MODE 1) for the boxes of one level -----------------------
-// Matrices are stored transposed (k-major) so lanes over output rows coalesce.
+// ---- leaf far field: coefficient records, then L2P + M2P -------------------------
+template <int P, class T>
+int launch_far(Handle& h, const double* M, const double* L, double* far, bool pot) {
+    using Lo = EvalLayout<P>;
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    T *hrec, *grec;
+    OGX_TRY(arena_get(h.ws, S_EVAL_H, (size_t)tv.nb * Lo::HREC, &hrec));
+    OGX_TRY(arena_get(h.ws, S_EVAL_G, (size_t)tv.nleaf * Lo::GREC, &grec));
+    k_eval_coeffs<P, 0, T><<<(tv.nb + 3) / 4, 128, 0, st>>>(tv, tv.nb, M, hrec); ++h.launches;
+    k_eval_coeffs<P, 1, T><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, tv.nleaf, L, grec); ++h.launches;
+    if (pot) { k_leaf_far<P, true, T><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hrec, grec, far); ++h.launches; }
+    else { k_leaf_far<P, false, T><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hrec, grec, far); ++h.launches; }
+    return OGX_OK;
+}
+
+// ---- M2M (MODE 0) / L2L (MODE 1) over the parents of one level ---------------------
+// CTA = 64 parents (8 warps x 8).  The CTA walks the child octants s = 0..7 and
+// stages the operator MM_s / LL_s (transposed, k-major) in shared memory once per
+// octant (orders with K*K*8 <= 100 KB; larger ones read it through L1), then every
+// warp applies it to its parents with lanes over the output dofs.
+//   M2M: M'_P = sum_s MM_s M'_{child s}                (src3d/AdaptiveFMM3D.hpp:62-71)
+//   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
+constexpr int TT_PAR = 8;   // parents per warp
+template <int P>
+constexpr bool tt_staged() { return (P + 1) * (P + 1) * (P + 1) * (P + 1) * 8 <= 100 * 1024; }
+template <int P>
+constexpr size_t tt_smem() {
+    return (size_t)(8 * TT_PAR) * (P + 1) * (P + 1) * 8 + (tt_staged<P>() ? (size_t)(P + 1) * (P + 1) * (P + 1) * (P + 1) * 8 : 0);
+}
+
 template <int P, int MODE>
-__global__ void __launch_bounds__(128) k_translate_level(TreeView tv, int first, int count, const double* opsT,
-                                                         double* mpole, double* local, const double* lown) {
+__global__ void __launch_bounds__(256) k_translate_tile(TreeView tv, int first, int count, const double* __restrict__ opsT,
+                                                        double* mpole, double* local, const double* __restrict__ lown) {
     constexpr int K = (P + 1) * (P + 1);
     constexpr int NPL = (K + 31) / 32;
-    __shared__ double s_vec[4][K];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int k = blockIdx.x * 4 + wid;
-    if (k >= count) return;
-    const int b = first + k;
-    double acc[NPL];
+    constexpr bool STAGED = tt_staged<P>();
+    extern __shared__ __align__(16) double s_dyn[];
+    double* s_in = s_dyn;                       // [64][K]
+    double* s_mat = s_dyn + 8 * TT_PAR * K;     // [K][K] when staged
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int bx[TT_PAR];
+    bool ok[TT_PAR];
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) acc[q] = 0.0;
-    if (MODE == 0) {
-        if (tv.leafid[b] >= 0) return;
-        for (int s = 0; s < 8; ++s) {
-            const int c = tv.child[8 * b + s];
-            if (c < 0) continue;
-            for (int d = lane; d < K; d += 32) s_vec[wid][d] = mpole[(size_t)c * K + d];
-            __syncwarp();
-            const double* T = opsT + (size_t)s * K * K;
+    for (int a = 0; a < TT_PAR; ++a) {
+        const int k = blockIdx.x * (8 * TT_PAR) + w * TT_PAR + a;
+        bx[a] = first + k;
+        ok[a] = (k < count) && (tv.leafid[bx[a]] < 0);
+    }
+    double acc[TT_PAR][NPL];
+#pragma unroll
+    for (int a = 0; a < TT_PAR; ++a)
+#pragma unroll
+        for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
+    if (MODE == 1) {
+#pragma unroll
+        for (int a = 0; a < TT_PAR; ++a)
+            for (int d = lane; d < K; d += 32) s_in[(w * TT_PAR + a) * K + d] = ok[a] ? local[(size_t)bx[a] * K + d] : 0.0;
+    }
+    for (int s = 0; s < 8; ++s) {
+        int ch[TT_PAR];
+        bool mine = false;
+#pragma unroll
+        for (int a = 0; a < TT_PAR; ++a) {
+            ch[a] = ok[a] ? tv.child[8 * bx[a] + s] : -1;
+            mine |= ch[a] >= 0;
+        }
+        if (!__syncthreads_or(mine)) continue;  // no parent of this CTA has child s
+        if (MODE == 0) {
+#pragma unroll
+            for (int a = 0; a < TT_PAR; ++a)
+                for (int d = lane; d < K; d += 32)
+                    s_in[(w * TT_PAR + a) * K + d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
+        } else {
+#pragma unroll
+            for (int a = 0; a < TT_PAR; ++a)
+#pragma unroll
+                for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
+        }
+        const double* T = opsT + (size_t)s * K * K;
+        if (STAGED) {
+            // scalar loads: T starts at s*K*K doubles, which is not 16-byte aligned for odd K*K
+            for (int i = threadIdx.x; i < K * K; i += blockDim.x) s_mat[i] = __ldg(T + i);
+        }
+        __syncthreads();
+        if (__any_sync(0xffffffffu, mine)) {
+            const double* Tm = STAGED ? s_mat : T;
             for (int kk = 0; kk < K; ++kk) {
-                const double v = s_vec[wid][kk];
+                double tq[NPL];
 #pragma unroll
                 for (int q = 0; q < NPL; ++q) {
                     const int j = lane + 32 * q;
-                    if (j < K) acc[q] = fma(__ldg(T + (size_t)kk * K + j), v, acc[q]);
+                    tq[q] = (j < K) ? (STAGED ? Tm[kk * K + j] : __ldg(Tm + (size_t)kk * K + j)) : 0.0;
+                }
+#pragma unroll
+                for (int a = 0; a < TT_PAR; ++a) {
+                    const double v = s_in[(w * TT_PAR + a) * K + kk];
+#pragma unroll
+                    for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
                 }
             }
-            __syncwarp();
         }
+        if (MODE == 1) {
 #pragma unroll
-        for (int q = 0; q < NPL; ++q) {
-            const int j = lane + 32 * q;
-            if (j < K) mpole[(size_t)b * K + j] = acc[q];
+            for (int a = 0; a < TT_PAR; ++a) {
+                if (ch[a] < 0) continue;
+#pragma unroll
+                for (int q = 0; q < NPL; ++q) {
+                    const int j = lane + 32 * q;
+                    if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
+                }
+            }
         }
-    } else {
-        const int P_ = tv.parent[b];
-        if (P_ < 0) {
-            for (int d = lane; d < K; d += 32) local[(size_t)b * K + d] = lown[(size_t)b * K + d];
-            return;
-        }
-        const int s = (tv.coord[3 * b] & 1) | ((tv.coord[3 * b + 1] & 1) << 1) | ((tv.coord[3 * b + 2] & 1) << 2);
-        for (int d = lane; d < K; d += 32) s_vec[wid][d] = local[(size_t)P_ * K + d];
-        __syncwarp();
-        const double* T = opsT + (size_t)s * K * K;
-        for (int kk = 0; kk < K; ++kk) {
-            const double v = s_vec[wid][kk];
+        __syncthreads();  // s_in / s_mat are rewritten for the next octant
+    }
+    if (MODE == 0) {
+#pragma unroll
+        for (int a = 0; a < TT_PAR; ++a) {
+            if (!ok[a]) continue;
 #pragma unroll
             for (int q = 0; q < NPL; ++q) {
                 const int j = lane + 32 * q;
-                if (j < K) acc[q] = fma(__ldg(T + (size_t)kk * K + j), v, acc[q]);
+                if (j < K) mpole[(size_t)bx[a] * K + j] = acc[a][q];
             }
         }
-#pragma unroll
-        for (int q = 0; q < NPL; ++q) {
-            const int j = lane + 32 * q;
-            if (j < K) local[(size_t)b * K + j] = lown[(size_t)b * K + j] + acc[q];
-        }
     }
+}
+
+template <int P>
+int launch_m2m(Handle& h, double* M) {
+    constexpr size_t smem = tt_smem<P>();
+    OGX_CUDA(cudaFuncSetAttribute(k_translate_tile<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int l = h.max_level - 1; l >= 0; --l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) { k_translate_tile<P, 0><<<(count + 8 * TT_PAR - 1) / (8 * TT_PAR), 256, smem, h.stream>>>(h.tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+    }
+    return OGX_OK;
+}
+
+template <int P>
+int launch_l2l(Handle& h, double* L, const double* Lown) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr size_t smem = tt_smem<P>();
+    OGX_CUDA(cudaFuncSetAttribute(k_translate_tile<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // root (no parent): its local is its own M2L/P2L part
+    OGX_CUDA(cudaMemcpyAsync(L + (size_t)h.level_off[0] * K, Lown + (size_t)h.level_off[0] * K, sizeof(double) * K,
+                             cudaMemcpyDeviceToDevice, h.stream));
+    for (int l = 0; l < h.max_level; ++l) {
+        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
+        if (count > 0) { k_translate_tile<P, 1><<<(count + 8 * TT_PAR - 1) / (8 * TT_PAR), 256, smem, h.stream>>>(h.tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+    }
+    return OGX_OK;
 }
 
 // ---- M2L (structured, FP64) -----------------------------------------------------------
@@ -239,10 +329,7 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     k_p2x<P, 0, double><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
-    for (int l = h.max_level - 1; l >= 0; --l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
-    }
+    OGX_TRY(launch_m2m<P>(h, M));
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
     // M2L
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
@@ -257,15 +344,11 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     k_p2x<P, 1, double><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
     // L2L top-down
-    for (int l = 0; l <= h.max_level; ++l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
-    }
+    OGX_TRY(launch_l2l<P>(h, L, Lown));
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     // leaves
     const bool pot = d_pot != nullptr;
-    if (pot) { k_leaf_far<P, true, double><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
-    else { k_leaf_far<P, false, double><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    OGX_TRY((launch_far<P, double>(h, M, L, far, pot)));
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
     if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
     else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
@@ -353,10 +436,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     k_p2x<P, 0, float><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
-    for (int l = h.max_level - 1; l >= 0; --l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_level<P, 0><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
-    }
+    OGX_TRY(launch_m2m<P>(h, M));
     {
         const int64_t tot = (int64_t)tv.nb * C::KPAD;
         if constexpr (C::SUPPORTED) { mixed::k_split_mpole<P><<<(int)((tot + 255) / 256), 256, 0, st>>>(M, tv.nb, mhi, mlo); ++h.launches; }
@@ -384,14 +464,10 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaEventRecord(h.ev[4], st));
     k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
-    for (int l = 0; l <= h.max_level; ++l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_level<P, 1><<<(count + 3) / 4, 128, 0, st>>>(tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
-    }
+    OGX_TRY(launch_l2l<P>(h, L, Lown));
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     const bool pot = d_pot != nullptr;
-    if (pot) { k_leaf_far<P, true, float><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
-    else { k_leaf_far<P, false, float><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, M, L, far); ++h.launches; }
+    OGX_TRY((launch_far<P, float>(h, M, L, far, pot)));
     const double G = h.prm.G;
     const float eps2 = (float)(h.prm.eps * h.prm.eps);
     if (pot) { mixed::k_leaf_near32<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }

@@ -74,7 +74,7 @@ enum Slot {
     S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, S_TGT_TILE, S_TGT_PKEY, S_TGT_PBOX,
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
-    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR,
+    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NUM_SLOTS
 };
 

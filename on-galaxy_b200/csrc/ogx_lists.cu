@@ -1,0 +1,329 @@
+// ogx_lists.cu -- Carrier-Greengard-Rokhlin interaction lists on the GPU.
+//
+// Replaces AdaptiveOctree::buildLists (src3d/AdaptiveOctree.hpp:137-189):
+//  - colleagues: same-level adjacent boxes, taken from the children of the
+//    parent's colleagues (:143-151).  Parent-centric: a warp per parent, lanes
+//    over its 27 colleague slots, each lane places the children of its
+//    colleague into the children's slots (slot = integer offset in [-1,1]^3);
+//  - V is implicit: children of the parent's colleagues at integer offset
+//    max|o| >= 2 (:154-161); every candidate is also classified with the
+//    reference's FP64 predicate and disagreements are counted (expected 0);
+//  - U/W per leaf (:164-169 with collectAdjLeaves :176-180 and descendW
+//    :181-189): warp per leaf, lane d owns colleague slot d: the slot's leaf
+//    (same level), the slot of every ancestor (coarser adjacent leaves) and a
+//    bounded explicit-stack descent of the slot's non-leaf colleague (finer U
+//    members and the W boxes).  A count pass sizes the CSR, a fill pass writes
+//    each lane's items at its warp-scan offset, so the order is deterministic;
+//  - X = transpose of W through a stable sort by W member (:171-173).
+#include "ogx_tree_common.cuh"
+
+namespace ogx {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int UW_STACK = 192;
+
+__global__ void k_root_col(int* col) {
+    const int d = threadIdx.x;
+    if (d < 27) col[d] = (d == 13) ? 0 : -1;
+}
+
+__global__ void __launch_bounds__(128) k_colleagues_par(int first, int count, const int* __restrict__ leafid,
+                                                        const int* __restrict__ child, const double* __restrict__ ctr,
+                                                        const RootInfo* root, int* col, DevCounts* counts) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = blockIdx.x * 4 + wid;
+    if (k >= count) return;
+    const int P = first + k;
+    if (leafid[P] >= 0) return;
+    int kids[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) kids[t] = child[8 * P + t];
+    const double tol = root->tol;
+    int mism = 0, nv = 0;
+    if (lane < 27) {
+        const int D = lane;
+        const int Q = col[27 * P + D];
+        if (Q >= 0) {
+            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+            for (int s = 0; s < 8; ++s) {
+                const int c = child[8 * Q + s];
+                if (c < 0) continue;
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const int b = kids[t];
+                    if (b < 0) continue;
+                    const int ox = 2 * Dx + (s & 1) - (t & 1), oy = 2 * Dy + ((s >> 1) & 1) - ((t >> 1) & 1),
+                              oz = 2 * Dz + ((s >> 2) & 1) - ((t >> 2) & 1);
+                    const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
+                    if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
+                    if (adj_i) col[27 * b + colleague_slot(ox, oy, oz)] = c;
+                    else ++nv;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mism += __shfl_xor_sync(FULL, mism, o);
+        nv += __shfl_xor_sync(FULL, nv, o);
+    }
+    if (lane == 0) {
+        if (mism) atomicAdd((unsigned long long*)&counts->adj_mismatch, (unsigned long long)mism);
+        if (nv) atomicAdd((unsigned long long*)&counts->v_total, (unsigned long long)nv);
+    }
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane) {
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    return x - v;
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restrict__ leafbox, const int* __restrict__ parent,
+                                                 const int* __restrict__ child, const int* __restrict__ leafid,
+                                                 const int* __restrict__ col, const double* __restrict__ ctr,
+                                                 const int* __restrict__ pcount, const RootInfo* root, int* lane_u, int* lane_w,
+                                                 int* ucnt, int* wcnt, const int64_t* uoff, const int64_t* woff, int* uidx,
+                                                 int* widx, DevCounts* counts) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= nleaf) return;
+    const int b = leafbox[lf];
+    const double tol = root->tol;
+    int nu = 0, nw = 0;
+    int64_t upairs = 0, ub = 0, wb = 0;
+    bool overflow = false;
+    if (FILL) {
+        ub = uoff[lf] + warp_excl_scan(lane_u[32 * lf + lane], lane);
+        wb = woff[lf] + warp_excl_scan(lane_w[32 * lf + lane], lane);
+    }
+    auto addU = [&](int c) {
+        if (FILL) uidx[ub + nu] = c;
+        else upairs += pcount[c];
+        ++nu;
+    };
+    if (lane < 27) {
+        const int d = lane;
+        const int c = col[27 * b + d];
+        if (c >= 0 && leafid[c] >= 0) addU(c);  // same-level adjacent leaves (b itself in slot 13)
+        for (int A = parent[b]; A >= 0; A = parent[A]) {  // coarser adjacent leaves
+            const int a2 = col[27 * A + d];
+            if (a2 >= 0 && leafid[a2] >= 0 && adjacent64(ctr, a2, b, tol)) addU(a2);
+        }
+        if (c >= 0 && c != b && leafid[c] < 0) {  // finer: descend the non-leaf colleague
+            int stk[UW_STACK];
+            int sp = 0;
+            stk[sp++] = c;
+            while (sp > 0) {
+                const int node = stk[--sp];
+                for (int s = 0; s < 8; ++s) {
+                    const int ch = child[8 * node + s];
+                    if (ch < 0) continue;
+                    if (!adjacent64(ctr, ch, b, tol)) {
+                        if (FILL) widx[wb + nw] = ch;
+                        ++nw;
+                    } else if (leafid[ch] >= 0) {
+                        addU(ch);
+                    } else if (sp < UW_STACK) {
+                        stk[sp++] = ch;
+                    } else {
+                        overflow = true;
+                    }
+                }
+            }
+        }
+    }
+    if (!FILL) {
+        lane_u[32 * lf + lane] = nu;
+        lane_w[32 * lf + lane] = nw;
+        int tu = nu, tw = nw;
+        int64_t tp = upairs;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            tu += __shfl_xor_sync(FULL, tu, o);
+            tw += __shfl_xor_sync(FULL, tw, o);
+            tp += __shfl_xor_sync(FULL, tp, o);
+        }
+        const bool any_over = __any_sync(FULL, overflow);
+        if (lane == 0) {
+            ucnt[lf] = tu;
+            wcnt[lf] = tw;
+            const int64_t pb = pcount[b];
+            atomicAdd((unsigned long long*)&counts->p2p_pairs, (unsigned long long)(pb * tp - pb));
+            atomicAdd((unsigned long long*)&counts->m2p_evals, (unsigned long long)(pb * tw));
+            atomicAdd((unsigned long long*)&counts->p2l_evals, (unsigned long long)(pb * tw));
+            if (any_over) atomicAdd((unsigned long long*)&counts->adj_mismatch, 1ull << 40);
+        }
+    }
+}
+
+// X = transpose of W: emit (w, leaf box) in leaf order, count members per box
+__global__ void k_x_emit(int nleaf, const int* leafbox, const int64_t* woff, const int* widx, uint32_t* xkey, uint32_t* xval,
+                         int* xcnt) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= nleaf) return;
+    const int b = leafbox[lf];
+    for (int64_t e = woff[lf]; e < woff[lf + 1]; ++e) {
+        xkey[e] = (uint32_t)widx[e];
+        xval[e] = (uint32_t)b;
+        atomicAdd(&xcnt[widx[e]], 1);
+    }
+}
+
+// M2L targets: boxes of level >= 2 keyed by their child octant
+__global__ void k_tgt_keys(int first, int nb, const int* coord, uint32_t* key, uint32_t* val) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb - first) return;
+    const int b = first + k;
+    key[k] = (uint32_t)((coord[3 * b] & 1) | ((coord[3 * b + 1] & 1) << 1) | ((coord[3 * b + 2] & 1) << 2));
+    val[k] = (uint32_t)b;
+}
+
+// padded per-octant layout of the M2L targets: every octant group starts on a
+// multiple of `tile`, so a tile never mixes octants.  gs[0..8] = group starts,
+// gs[9..17] = padded group starts.
+__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int* gs) {
+    __shared__ int lo_s[9];
+    const int g = threadIdx.x;
+    if (g <= 8) {
+        int lo = 0, hi = ntgt;  // first index with key >= g
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)key[mid] < g) lo = mid + 1; else hi = mid;
+        }
+        lo_s[g] = lo;
+        gs[g] = lo;
+    }
+    __syncthreads();
+    if (g == 0) {
+        int pad = 0;
+        for (int q = 0; q <= 8; ++q) {
+            gs[9 + q] = pad;
+            if (q < 8) pad += ((lo_s[q + 1] - lo_s[q] + tile - 1) / tile) * tile;
+        }
+    }
+}
+__global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, uint32_t* pkey, uint32_t* pbox) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npad) return;
+    uint32_t k = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
+    for (int g = 0; g < 8; ++g) {
+        const int ps = gs[9 + g], pe = gs[9 + g + 1];
+        if (q >= ps && q < pe) {
+            const int local = q - ps;
+            if (local < gs[g + 1] - gs[g]) { k = (uint32_t)g; b = box[gs[g] + local]; }
+            break;
+        }
+    }
+    pkey[q] = k;
+    pbox[q] = b;
+}
+
+inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
+inline int bits_for(int64_t v) {
+    int b = 1;
+    while ((1ll << b) <= v) ++b;
+    return b;
+}
+
+}  // namespace
+
+int lists_build(Handle& h) {
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    const int nb = tv.nb, nleaf = tv.nleaf;
+    DevCounts* dc;
+    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    int* col;
+    OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
+    OGX_CUDA(cudaMemsetAsync(col, 0xFF, 27 * sizeof(int) * (size_t)nb, st));
+    k_root_col<<<1, 32, 0, st>>>(col); ++h.launches;
+    for (int l = 1; l <= h.max_level; ++l) {
+        const int first = h.level_off[l - 1], count = h.level_off[l] - first;
+        k_colleagues_par<<<grid_for(count, 4), 128, 0, st>>>(first, count, tv.leafid, tv.child, tv.center, tv.root, col, dc); ++h.launches;
+    }
+    tv.col = col;
+
+    int *ucnt, *wcnt, *lane_uw;
+    int64_t *uoff, *woff;
+    OGX_TRY(arena_get(h.ws, S_U_CNT, nleaf, &ucnt));
+    OGX_TRY(arena_get(h.ws, S_W_CNT, nleaf, &wcnt));
+    OGX_TRY(arena_get(h.ws, S_UW_LANE, 64 * (size_t)nleaf, &lane_uw));
+    OGX_TRY(arena_get(h.ws, S_U_OFF, nleaf + 1, &uoff));
+    OGX_TRY(arena_get(h.ws, S_W_OFF, nleaf + 1, &woff));
+    int* lane_u = lane_uw;
+    int* lane_w = lane_uw + 32 * (size_t)nleaf;
+    k_uw_warp<false><<<grid_for(nleaf, 4), 128, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center,
+                                                         tv.pcount, tv.root, lane_u, lane_w, ucnt, wcnt, nullptr, nullptr,
+                                                         nullptr, nullptr, dc); ++h.launches;
+    OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
+    OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
+    // sync point 2: list sizes
+    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->u_total, uoff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->w_total, woff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaStreamSynchronize(st));
+    const int64_t nu = h.h_counts->u_total, nw = h.h_counts->w_total;
+    int *uidx, *widx;
+    OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
+    OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));
+    k_uw_warp<true><<<grid_for(nleaf, 4), 128, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center,
+                                                        tv.pcount, tv.root, lane_u, lane_w, nullptr, nullptr, uoff, woff, uidx,
+                                                        widx, dc); ++h.launches;
+    tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
+
+    // X lists
+    uint32_t *xk, *xv;
+    int* xcnt;
+    int64_t* xoff;
+    OGX_TRY(arena_get(h.ws, S_X_KEY, nw + 1, &xk));
+    OGX_TRY(arena_get(h.ws, S_X_VAL, nw + 1, &xv));
+    OGX_TRY(arena_get(h.ws, S_X_CNT, nb, &xcnt));
+    OGX_TRY(arena_get(h.ws, S_X_OFF, nb + 1, &xoff));
+    OGX_CUDA(cudaMemsetAsync(xcnt, 0, sizeof(int) * (size_t)nb, st));
+    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt); ++h.launches;
+    uint32_t *xk_s, *xv_s;
+    OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, bits_for(nb), &xk_s, &xv_s));
+    OGX_TRY(scan_i32_to_i64(h, xcnt, xoff, nb));
+    tv.x_off = xoff;
+    tv.x_idx = (const int*)xv_s;
+
+    // M2L targets grouped by child octant (levels >= 2)
+    const int first2 = (h.max_level >= 2) ? h.level_off[2] : nb;
+    const int ntgt = nb - first2;
+    uint32_t *tk, *tb;
+    OGX_TRY(arena_get(h.ws, S_TGT_KEY, ntgt + 1, &tk));
+    OGX_TRY(arena_get(h.ws, S_TGT_BOX, ntgt + 1, &tb));
+    if (ntgt > 0) {
+        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tk, tb); ++h.launches;
+        uint32_t *tk_s, *tb_s;
+        OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 3, &tk_s, &tb_s));
+        h.tgt_key = tk_s;
+        h.tgt_box = tb_s;
+        const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
+        const int npad = ((ntgt + tile - 1) / tile + 8) * tile;
+        int* gs;
+        uint32_t *pk, *pb;
+        OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
+        OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
+        OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
+        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs); ++h.launches;
+        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb); ++h.launches;
+        h.tgt_tile_key = pk;
+        h.tgt_tile_box = pb;
+        h.ntgt_pad = npad;
+    } else {
+        h.ntgt_pad = 0;
+    }
+    h.ntgt = ntgt;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+}  // namespace ogx

@@ -64,33 +64,64 @@ __global__ void __launch_bounds__(RS_THREADS) rs_hist(KO keys, int64_t n, int pa
     hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// exclusive scan of m uint32 values in place, one block of 1024 threads
-__global__ void __launch_bounds__(1024) rs_scan(uint32_t* a, int64_t m) {
-    __shared__ uint32_t part[1024];
-    const int t = threadIdx.x;
-    const int64_t per = (m + 1023) / 1024;
-    const int64_t b = t * per, e = min(m, b + per);
-    uint32_t s = 0;
-    for (int64_t i = b; i < e; ++i) s += a[i];
-    part[t] = s;
+// Digit-major histogram hist[d * nblocks + b] -> exclusive offsets within each digit
+// (one CTA per digit, coalesced over the tiles), digit totals into tot[d].
+__global__ void __launch_bounds__(1024) rs_scan_digit(uint32_t* hist, int nblocks, uint32_t* tot) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t carry;
+    uint32_t* a = hist + (size_t)blockIdx.x * nblocks;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) carry = 0;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        uint32_t v = (t >= off) ? part[t - off] : 0;
+    for (int b0 = 0; b0 < nblocks; b0 += 1024) {
+        const int i = b0 + t;
+        const uint32_t v = (i < nblocks) ? a[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sum[w] = x;
         __syncthreads();
-        part[t] += v;
+        if (w == 0) {
+            uint32_t s = warp_sum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, s, o);
+                if (lane >= o) s += y;
+            }
+            warp_sum[lane] = s;
+        }
+        __syncthreads();
+        const uint32_t ex = carry + (w > 0 ? warp_sum[w - 1] : 0u) + x - v;
+        if (i < nblocks) a[i] = ex;
+        __syncthreads();
+        if (t == 0) carry += warp_sum[31];
         __syncthreads();
     }
-    uint32_t run = part[t] - s;
-    for (int64_t i = b; i < e; ++i) {
-        const uint32_t v = a[i];
-        a[i] = run;
-        run += v;
+    if (t == 0) tot[blockIdx.x] = carry;
+}
+
+// exclusive scan of the 256 digit totals (in place)
+__global__ void __launch_bounds__(256) rs_scan_totals(uint32_t* tot) {
+    __shared__ uint32_t s[256];
+    const int t = threadIdx.x;
+    const uint32_t v = tot[t];
+    s[t] = v;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        const uint32_t y = (t >= o) ? s[t - o] : 0u;
+        __syncthreads();
+        s[t] += y;
+        __syncthreads();
     }
+    tot[t] = s[t] - v;
 }
 
 template <class KO>
 __global__ void __launch_bounds__(RS_THREADS) rs_scatter(KO kin, KO kout, const uint32_t* vin, uint32_t* vout, int64_t n,
-                                                         int pass, const uint32_t* scanned, int nblocks) {
+                                                         int pass, const uint32_t* scanned, int nblocks, const uint32_t* digit_base) {
     __shared__ uint32_t wcnt[RS_WARPS][256];
     __shared__ uint32_t gbase[256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -129,7 +160,7 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(KO kin, KO kout, const 
             wcnt[ww][d] = run;
             run += c;
         }
-        gbase[d] = scanned[(int64_t)d * nblocks + blockIdx.x];
+        gbase[d] = digit_base[d] + scanned[(int64_t)d * nblocks + blockIdx.x];
     }
     __syncthreads();
 #pragma unroll
@@ -247,13 +278,15 @@ template <class KO>
 static int radix_passes(Handle& h, KO a, KO b, uint32_t* va, uint32_t* vb, int64_t n, int npasses, int* which) {
     const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
     uint32_t* hist;
-    OGX_TRY(arena_get(h.ws, S_RS_HIST, (size_t)256 * nblocks, &hist));
+    OGX_TRY(arena_get(h.ws, S_RS_HIST, (size_t)256 * nblocks + 256, &hist));
+    uint32_t* tot = hist + (size_t)256 * nblocks;
     KO src = a, dst = b;
     uint32_t *vs = va, *vd = vb;
     for (int pass = 0; pass < npasses; ++pass) {
         rs_hist<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, n, pass, hist, nblocks); ++h.launches;
-        rs_scan<<<1, 1024, 0, h.stream>>>(hist, (int64_t)256 * nblocks); ++h.launches;
-        rs_scatter<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, dst, vs, vd, n, pass, hist, nblocks); ++h.launches;
+        rs_scan_digit<<<256, 1024, 0, h.stream>>>(hist, nblocks, tot); ++h.launches;
+        rs_scan_totals<<<1, 256, 0, h.stream>>>(tot); ++h.launches;
+        rs_scatter<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, dst, vs, vd, n, pass, hist, nblocks, tot); ++h.launches;
         std::swap(src, dst);
         std::swap(vs, vd);
     }

@@ -30,7 +30,7 @@
 //    come from the colleague slots of the leaf and its ancestors, finer ones
 //    from a bounded explicit-stack descent of non-leaf colleagues;
 //  - X = transpose of W via a stable sort (:171-173).
-#include "ogx_internal.cuh"
+#include "ogx_tree_common.cuh"
 
 namespace ogx {
 namespace {
@@ -67,11 +67,25 @@ __global__ void k_bbox_partial(const double* pos, int64_t n, double* part) {
 }
 
 // AdaptiveOctree::build :71-81; eps-floor level from subdivide :102
-__global__ void k_bbox_final(const double* part, int nparts, double eps_floor, RootInfo* root) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(256) k_bbox_final(const double* part, int nparts, double eps_floor, RootInfo* root) {
+    __shared__ double sh[8][6];
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int b = 0; b < nparts; ++b)
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
         for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], part[6 * b + a]); hi[a] = fmax(hi[a], part[6 * b + 3 + a]); }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fmin(lo[a], __shfl_xor_sync(FULL, lo[a], o));
+            hi[a] = fmax(hi[a], __shfl_xor_sync(FULL, hi[a], o));
+        }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) { sh[w][a] = lo[a]; sh[w][3 + a] = hi[a]; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww)
+        for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], sh[ww][a]); hi[a] = fmax(hi[a], sh[ww][3 + a]); }
+    for (int a = 0; a < 3; ++a) { lo[a] = fmin(lo[a], sh[0][a]); hi[a] = fmax(hi[a], sh[0][3 + a]); }
     RootInfo r;
     for (int a = 0; a < 3; ++a) r.c[a] = __dmul_rn(0.5, __dadd_rn(lo[a], hi[a]));
     double ext = __dsub_rn(hi[0], lo[0]);
@@ -264,13 +278,12 @@ __global__ void k_boxes(int nb, const uint32_t* reclev, const uint32_t* recpos, 
     child[8 * lo_i + key_digit(hi, lo, l)] = k;
 }
 
-__global__ void k_pcount_up(int nleaf, const int* leafbox, const int* parent, int* pcount, DevCounts* counts) {
+__global__ void k_leaf_occupancy(int nleaf, const int* leafbox, const int* pcount, DevCounts* counts) {
     const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lf >= nleaf) return;
-    const int b = leafbox[lf];
-    const int c = pcount[b];
-    atomicMax(&counts->max_leaf_occ, c);
-    for (int a = parent[b]; a >= 0; a = parent[a]) atomicAdd(&pcount[a], c);
+    int c = (lf < nleaf) ? pcount[leafbox[lf]] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(FULL, c, o));
+    if ((threadIdx.x & 31) == 0 && c > 0) atomicMax(&counts->max_leaf_occ, c);
 }
 
 // ---- 5. final body order ----------------------------------------------------------
@@ -288,184 +301,6 @@ __global__ void k_gather_bodies(const uint32_t* perm, const double* pos, const d
     perm_out[i] = (int)j;
     px[i] = pos[3 * j]; py[i] = pos[3 * j + 1]; pz[i] = pos[3 * j + 2];
     pm[i] = mass[j];
-}
-
-// ---- lists ------------------------------------------------------------------------
-__device__ __forceinline__ bool adjacent64(const double* ctr, int a, int b, double tol) {
-    // AdaptiveOctree::adjacent (src3d/AdaptiveOctree.hpp:58-62)
-    const double s = __dadd_rn(__dadd_rn(ctr[4 * a + 3], ctr[4 * b + 3]), tol);
-    return fabs(__dsub_rn(ctr[4 * a], ctr[4 * b])) <= s && fabs(__dsub_rn(ctr[4 * a + 1], ctr[4 * b + 1])) <= s &&
-           fabs(__dsub_rn(ctr[4 * a + 2], ctr[4 * b + 2])) <= s;
-}
-
-__global__ void k_root_col(int* col) {
-    const int d = threadIdx.x;
-    if (d < 27) col[d] = (d == 13) ? 0 : -1;
-}
-
-// colleagues of the boxes of one level, from the parent's colleague slots
-__global__ void k_colleagues(int first, int count, const int* parent, const int* coord, const int* child, const double* ctr,
-                             const RootInfo* root, int* col, DevCounts* counts) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    const int b = first + k;
-    const int P = parent[b];
-    const int tx = coord[3 * b] & 1, ty = coord[3 * b + 1] & 1, tz = coord[3 * b + 2] & 1;
-    int mine[27];
-#pragma unroll
-    for (int d = 0; d < 27; ++d) mine[d] = -1;
-    const double tol = root->tol;
-    int mism = 0, nv = 0;
-    for (int D = 0; D < 27; ++D) {
-        const int Q = col[27 * P + D];
-        if (Q < 0) continue;
-        const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
-        for (int s = 0; s < 8; ++s) {
-            const int c = child[8 * Q + s];
-            if (c < 0) continue;
-            const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
-            const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
-            if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
-            nv += !adj_i;
-            if (adj_i) mine[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] = c;
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 27; ++d) col[27 * b + d] = mine[d];
-    if (mism) atomicAdd((unsigned long long*)&counts->adj_mismatch, (unsigned long long)mism);
-    if (nv) atomicAdd((unsigned long long*)&counts->v_total, (unsigned long long)nv);
-}
-
-constexpr int UW_STACK = 256;
-
-// U and W of one leaf (AdaptiveOctree::buildLists :164-169 with collectAdjLeaves
-// :176-180 and descendW :181-189).  FILL=false counts, FILL=true writes.
-template <bool FILL>
-__global__ void k_uw(int nleaf, const int* leafbox, const int* parent, const int* child, const int* leafid, const int* col,
-                     const double* ctr, const int* pcount, const RootInfo* root, int* ucnt, int* wcnt, const int64_t* uoff,
-                     const int64_t* woff, int* uidx, int* widx, DevCounts* counts) {
-    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lf >= nleaf) return;
-    const int b = leafbox[lf];
-    const double tol = root->tol;
-    int64_t nu = 0, nw = 0;
-    int64_t ub = FILL ? uoff[lf] : 0, wb = FILL ? woff[lf] : 0;
-    int64_t upairs = 0;
-    auto addU = [&](int c) {
-        if (FILL) uidx[ub + nu] = c;
-        ++nu;
-        if (!FILL) upairs += pcount[c];
-    };
-    // same level (includes b itself)
-    for (int d = 0; d < 27; ++d) {
-        const int c = col[27 * b + d];
-        if (c >= 0 && leafid[c] >= 0) addU(c);
-    }
-    // coarser adjacent leaves: colleagues of ancestors
-    for (int A = parent[b]; A >= 0; A = parent[A])
-        for (int d = 0; d < 27; ++d) {
-            const int c = col[27 * A + d];
-            if (c >= 0 && leafid[c] >= 0 && adjacent64(ctr, c, b, tol)) addU(c);
-        }
-    // finer: descend non-leaf colleagues
-    int stk[UW_STACK];
-    int sp = 0;
-    bool overflow = false;
-    for (int d = 0; d < 27; ++d) {
-        const int c = col[27 * b + d];
-        if (c < 0 || c == b || leafid[c] >= 0) continue;
-        stk[sp++] = c;
-        while (sp > 0) {
-            const int node = stk[--sp];
-            for (int s = 0; s < 8; ++s) {
-                const int ch = child[8 * node + s];
-                if (ch < 0) continue;
-                if (!adjacent64(ctr, ch, b, tol)) {
-                    if (FILL) widx[wb + nw] = ch;
-                    ++nw;
-                } else if (leafid[ch] >= 0) {
-                    addU(ch);
-                } else if (sp < UW_STACK) {
-                    stk[sp++] = ch;
-                } else {
-                    overflow = true;
-                }
-            }
-        }
-    }
-    if (!FILL) {
-        ucnt[lf] = (int)nu;
-        wcnt[lf] = (int)nw;
-        const int64_t pb = pcount[b];
-        atomicAdd((unsigned long long*)&counts->p2p_pairs, (unsigned long long)(pb * upairs - pb));
-        atomicAdd((unsigned long long*)&counts->m2p_evals, (unsigned long long)(pb * nw));
-        atomicAdd((unsigned long long*)&counts->p2l_evals, (unsigned long long)(pb * nw));
-        if (overflow) atomicAdd((unsigned long long*)&counts->adj_mismatch, 1ull << 40);
-    }
-}
-
-// X = transpose of W: emit (w, leaf box) in leaf order, count members per box
-__global__ void k_x_emit(int nleaf, const int* leafbox, const int64_t* woff, const int* widx, uint32_t* xkey, uint32_t* xval,
-                         int* xcnt) {
-    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lf >= nleaf) return;
-    const int b = leafbox[lf];
-    for (int64_t e = woff[lf]; e < woff[lf + 1]; ++e) {
-        xkey[e] = (uint32_t)widx[e];
-        xval[e] = (uint32_t)b;
-        atomicAdd(&xcnt[widx[e]], 1);
-    }
-}
-
-// M2L targets: boxes of level >= 2 keyed by their child octant
-__global__ void k_tgt_keys(int first, int nb, const int* coord, uint32_t* key, uint32_t* val) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nb - first) return;
-    const int b = first + k;
-    key[k] = (uint32_t)((coord[3 * b] & 1) | ((coord[3 * b + 1] & 1) << 1) | ((coord[3 * b + 2] & 1) << 2));
-    val[k] = (uint32_t)b;
-}
-
-// padded per-octant layout of the M2L targets: every octant group starts on a
-// multiple of `tile`, so a tile never mixes octants
-__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int* gs) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    int pad = 0;
-    for (int g = 0; g <= 8; ++g) {
-        int lo = 0, hi = ntgt;  // first index with key >= g
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if ((int)key[mid] < g) lo = mid + 1; else hi = mid;
-        }
-        gs[g] = lo;
-        gs[9 + g] = pad;
-        if (g < 8) {
-            int cnt_hi = ntgt, l2 = 0;  // first index with key >= g+1
-            int a = 0, b2 = ntgt;
-            while (a < b2) {
-                const int mid = (a + b2) >> 1;
-                if ((int)key[mid] < g + 1) a = mid + 1; else b2 = mid;
-            }
-            cnt_hi = a;
-            l2 = cnt_hi - lo;
-            pad += ((l2 + tile - 1) / tile) * tile;
-        }
-    }
-}
-__global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, uint32_t* pkey, uint32_t* pbox) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= npad) return;
-    uint32_t k = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
-    for (int g = 0; g < 8; ++g) {
-        const int ps = gs[9 + g], pe = gs[9 + g + 1];
-        if (q >= ps && q < pe) {
-            const int local = q - ps;
-            if (local < gs[g + 1] - gs[g]) { k = (uint32_t)g; b = box[gs[g] + local]; }
-            break;
-        }
-    }
-    pkey[q] = k;
-    pbox[q] = b;
 }
 
 }  // namespace
@@ -491,7 +326,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCounts), st));
 
     k_bbox_partial<<<nparts, 256, 0, st>>>(d_pos, n, part); ++h.launches;
-    k_bbox_final<<<1, 32, 0, st>>>(part, nparts, h.prm.eps, root); ++h.launches;
+    k_bbox_final<<<1, 256, 0, st>>>(part, nparts, h.prm.eps, root); ++h.launches;
 
     uint64_t* khi;
     uint32_t *klo, *kidx;
@@ -555,7 +390,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_CUDA(cudaMemsetAsync(pcount, 0, sizeof(int) * (size_t)nb, st));
     k_boxes<<<grid_for(nb, 128), 128, 0, st>>>(nb, reclev, recpos_s, level_off_dev, khi, klo, leaflev, leafscan, leafstart, root,
                                                 level, coord, center, parent, child, leafid, pfirst, pcount, leafbox); ++h.launches;
-    k_pcount_up<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, parent, pcount, dc); ++h.launches;
+    k_leaf_occupancy<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, pcount, dc); ++h.launches;
 
     // final body order: stable by leaf id from the original order
     uint32_t *lk, *ident;
@@ -579,93 +414,6 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     tv.px = px; tv.py = py; tv.pz = pz; tv.pm = pm; tv.perm = perm;
     tv.level = level; tv.coord = coord; tv.center = center; tv.parent = parent; tv.child = child;
     tv.leafid = leafid; tv.pfirst = pfirst; tv.pcount = pcount; tv.leafbox = leafbox;
-    return OGX_OK;
-}
-
-int lists_build(Handle& h) {
-    const cudaStream_t st = h.stream;
-    TreeView& tv = h.tv;
-    const int nb = tv.nb, nleaf = tv.nleaf;
-    DevCounts* dc;
-    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
-    int* col;
-    OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
-    k_root_col<<<1, 32, 0, st>>>(col); ++h.launches;
-    for (int l = 1; l <= h.max_level; ++l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - h.level_off[l];
-        if (count > 0)
-            k_colleagues<<<grid_for(count, 128), 128, 0, st>>>(first, count, tv.parent, tv.coord, tv.child, tv.center, tv.root,
-                                                                 col, dc); ++h.launches;
-    }
-    tv.col = col;
-    int *ucnt, *wcnt;
-    int64_t *uoff, *woff;
-    OGX_TRY(arena_get(h.ws, S_U_CNT, nleaf, &ucnt));
-    OGX_TRY(arena_get(h.ws, S_W_CNT, nleaf, &wcnt));
-    OGX_TRY(arena_get(h.ws, S_U_OFF, nleaf + 1, &uoff));
-    OGX_TRY(arena_get(h.ws, S_W_OFF, nleaf + 1, &woff));
-    k_uw<false><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
-                                                     tv.root, ucnt, wcnt, nullptr, nullptr, nullptr, nullptr, dc); ++h.launches;
-    OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
-    OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
-    // sync point 2: list sizes
-    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->u_total, uoff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->w_total, woff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaStreamSynchronize(st));
-    const int64_t nu = h.h_counts->u_total, nw = h.h_counts->w_total;
-    int *uidx, *widx;
-    OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
-    OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));
-    k_uw<true><<<grid_for(nleaf, 64), 64, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center, tv.pcount,
-                                                    tv.root, nullptr, nullptr, uoff, woff, uidx, widx, dc); ++h.launches;
-    tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
-
-    // X lists
-    uint32_t *xk, *xv;
-    int* xcnt;
-    int64_t* xoff;
-    OGX_TRY(arena_get(h.ws, S_X_KEY, nw + 1, &xk));
-    OGX_TRY(arena_get(h.ws, S_X_VAL, nw + 1, &xv));
-    OGX_TRY(arena_get(h.ws, S_X_CNT, nb, &xcnt));
-    OGX_TRY(arena_get(h.ws, S_X_OFF, nb + 1, &xoff));
-    OGX_CUDA(cudaMemsetAsync(xcnt, 0, sizeof(int) * (size_t)nb, st));
-    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt); ++h.launches;
-    uint32_t *xk_s, *xv_s;
-    OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, bits_for(nb), &xk_s, &xv_s));
-    OGX_TRY(scan_i32_to_i64(h, xcnt, xoff, nb));
-    tv.x_off = xoff;
-    tv.x_idx = (const int*)xv_s;
-
-    // M2L targets grouped by child octant (levels >= 2)
-    const int first2 = (h.max_level >= 2) ? h.level_off[2] : nb;
-    const int ntgt = nb - first2;
-    uint32_t *tk, *tb;
-    OGX_TRY(arena_get(h.ws, S_TGT_KEY, ntgt + 1, &tk));
-    OGX_TRY(arena_get(h.ws, S_TGT_BOX, ntgt + 1, &tb));
-    if (ntgt > 0) {
-        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tk, tb); ++h.launches;
-        uint32_t *tk_s, *tb_s;
-        OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 3, &tk_s, &tb_s));
-        h.tgt_key = tk_s;
-        h.tgt_box = tb_s;
-        const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
-        const int npad = ((ntgt + tile - 1) / tile + 8) * tile;
-        int* gs;
-        uint32_t *pk, *pb;
-        OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
-        OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
-        OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
-        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs); ++h.launches;
-        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb); ++h.launches;
-        h.tgt_tile_key = pk;
-        h.tgt_tile_box = pb;
-        h.ntgt_pad = npad;
-    } else {
-        h.ntgt_pad = 0;
-    }
-    h.ntgt = ntgt;
-    OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
 
