@@ -48,113 +48,116 @@ int launch_far(Handle& h, const double* M, const double* L, double* far, bool po
     return OGX_OK;
 }
 
-// ---- M2M (MODE 0) / L2L (MODE 1) over the parents of one level ---------------------
-// CTA = 64 parents (8 warps x 8).  The CTA walks the child octants s = 0..7 and
-// stages the operator MM_s / LL_s (transposed, k-major) in shared memory once per
-// octant (orders with K*K*8 <= 100 KB; larger ones read it through L1), then every
-// warp applies it to its parents with lanes over the output dofs.
-//   M2M: M'_P = sum_s MM_s M'_{child s}                (src3d/AdaptiveFMM3D.hpp:62-71)
-//   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
-constexpr int TT_PAR = 8;   // parents per warp
+// mixed form: FP32 records with folded weights, flat (body, W box) M2P tasks
 template <int P>
-constexpr bool tt_staged() { return (P + 1) * (P + 1) * (P + 1) * (P + 1) * 8 <= 100 * 1024; }
-template <int P>
-constexpr size_t tt_smem() {
-    return (size_t)(8 * TT_PAR) * (P + 1) * (P + 1) * 8 + (tt_staged<P>() ? (size_t)(P + 1) * (P + 1) * (P + 1) * (P + 1) * 8 : 0);
+int launch_far32(Handle& h, const double* M, const double* L, double* far, bool pot) {
+    using R = mixed::FarRec32<P>;
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    float4 *hrec, *grec;
+    OGX_TRY(arena_get(h.ws, S_EVAL_H, (size_t)tv.nb * 2 * R::NEH, &hrec));
+    OGX_TRY(arena_get(h.ws, S_EVAL_G, (size_t)tv.nleaf * 2 * R::NEG, &grec));
+    mixed::k_far_rec32<P, 0><<<(tv.nb + 3) / 4, 128, 0, st>>>(tv, tv.nb, M, hrec); ++h.launches;
+    mixed::k_far_rec32<P, 1><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, tv.nleaf, L, grec); ++h.launches;
+    const size_t smem = mixed::far_smem_bytes<P>();
+    if (pot) {
+        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mixed::k_leaf_far32<P, true><<<(tv.nleaf + 3) / 4, 128, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+    } else {
+        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mixed::k_leaf_far32<P, false><<<(tv.nleaf + 3) / 4, 128, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+    }
+    return OGX_OK;
 }
 
+// ---- M2M (MODE 0) / L2L (MODE 1) over the non-leaf parents of one level ------------
+// CTA = TR_PB parents x 8 warps, warp s = child octant s.  Warp s applies the
+// operator MM_s / LL_s (transposed, k-major, L2-resident) to its TR_PB parents,
+// lanes over output dofs.
+//   M2M: M'_P = sum_s MM_s M'_{child s}                (src3d/AdaptiveFMM3D.hpp:62-71)
+//        the eight partial products are summed in octant order through shared memory
+//   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
+constexpr int TR_PB = 2;   // parents per CTA
 template <int P, int MODE>
-__global__ void __launch_bounds__(256) k_translate_tile(TreeView tv, int first, int count, const double* __restrict__ opsT,
-                                                        double* mpole, double* local, const double* __restrict__ lown) {
+__global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* __restrict__ parents, int count,
+                                                       const double* __restrict__ opsT, double* mpole, double* local,
+                                                       const double* __restrict__ lown) {
     constexpr int K = (P + 1) * (P + 1);
     constexpr int NPL = (K + 31) / 32;
-    constexpr bool STAGED = tt_staged<P>();
-    extern __shared__ __align__(16) double s_dyn[];
-    double* s_in = s_dyn;                       // [64][K]
-    double* s_mat = s_dyn + 8 * TT_PAR * K;     // [K][K] when staged
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int bx[TT_PAR];
-    bool ok[TT_PAR];
+    __shared__ double s_in[MODE == 0 ? 8 : 1][TR_PB][K];
+    __shared__ double s_part[MODE == 0 ? 8 : 1][TR_PB][MODE == 0 ? K : 1];
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const int p0 = blockIdx.x * TR_PB;
+    int bx[TR_PB], ch[TR_PB];
+    bool any = false;
 #pragma unroll
-    for (int a = 0; a < TT_PAR; ++a) {
-        const int k = blockIdx.x * (8 * TT_PAR) + w * TT_PAR + a;
-        bx[a] = first + k;
-        ok[a] = (k < count) && (tv.leafid[bx[a]] < 0);
-    }
-    double acc[TT_PAR][NPL];
-#pragma unroll
-    for (int a = 0; a < TT_PAR; ++a)
-#pragma unroll
-        for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
-    if (MODE == 1) {
-#pragma unroll
-        for (int a = 0; a < TT_PAR; ++a)
-            for (int d = lane; d < K; d += 32) s_in[(w * TT_PAR + a) * K + d] = ok[a] ? local[(size_t)bx[a] * K + d] : 0.0;
-    }
-    for (int s = 0; s < 8; ++s) {
-        int ch[TT_PAR];
-        bool mine = false;
-#pragma unroll
-        for (int a = 0; a < TT_PAR; ++a) {
-            ch[a] = ok[a] ? tv.child[8 * bx[a] + s] : -1;
-            mine |= ch[a] >= 0;
-        }
-        if (!__syncthreads_or(mine)) continue;  // no parent of this CTA has child s
-        if (MODE == 0) {
-#pragma unroll
-            for (int a = 0; a < TT_PAR; ++a)
-                for (int d = lane; d < K; d += 32)
-                    s_in[(w * TT_PAR + a) * K + d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
-        } else {
-#pragma unroll
-            for (int a = 0; a < TT_PAR; ++a)
-#pragma unroll
-                for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
-        }
-        const double* T = opsT + (size_t)s * K * K;
-        if (STAGED) {
-            // scalar loads: T starts at s*K*K doubles, which is not 16-byte aligned for odd K*K
-            for (int i = threadIdx.x; i < K * K; i += blockDim.x) s_mat[i] = __ldg(T + i);
-        }
-        __syncthreads();
-        if (__any_sync(0xffffffffu, mine)) {
-            const double* Tm = STAGED ? s_mat : T;
-            for (int kk = 0; kk < K; ++kk) {
-                double tq[NPL];
-#pragma unroll
-                for (int q = 0; q < NPL; ++q) {
-                    const int j = lane + 32 * q;
-                    tq[q] = (j < K) ? (STAGED ? Tm[kk * K + j] : __ldg(Tm + (size_t)kk * K + j)) : 0.0;
-                }
-#pragma unroll
-                for (int a = 0; a < TT_PAR; ++a) {
-                    const double v = s_in[(w * TT_PAR + a) * K + kk];
-#pragma unroll
-                    for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
-                }
-            }
-        }
-        if (MODE == 1) {
-#pragma unroll
-            for (int a = 0; a < TT_PAR; ++a) {
-                if (ch[a] < 0) continue;
-#pragma unroll
-                for (int q = 0; q < NPL; ++q) {
-                    const int j = lane + 32 * q;
-                    if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
-                }
-            }
-        }
-        __syncthreads();  // s_in / s_mat are rewritten for the next octant
+    for (int a = 0; a < TR_PB; ++a) {
+        bx[a] = (p0 + a < count) ? parents[p0 + a] : -1;
+        ch[a] = (bx[a] >= 0) ? tv.child[8 * bx[a] + s] : -1;
+        any |= ch[a] >= 0;
     }
     if (MODE == 0) {
 #pragma unroll
-        for (int a = 0; a < TT_PAR; ++a) {
-            if (!ok[a]) continue;
+        for (int a = 0; a < TR_PB; ++a)
+            for (int d = lane; d < K; d += 32) s_in[s][a][d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
+        __syncwarp();
+    } else {
+#pragma unroll
+        for (int a = 0; a < TR_PB; ++a)
+            for (int d = threadIdx.x; d < K; d += blockDim.x) s_in[0][a][d] = (bx[a] >= 0) ? local[(size_t)bx[a] * K + d] : 0.0;
+        __syncthreads();
+    }
+    double acc[TR_PB][NPL];
+#pragma unroll
+    for (int a = 0; a < TR_PB; ++a)
+#pragma unroll
+        for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
+    if (any) {  // warp-uniform
+        const double* T = opsT + (size_t)s * K * K;
+        const int si = MODE == 0 ? s : 0;
+#pragma unroll 4
+        for (int kk = 0; kk < K; ++kk) {
+            double tq[NPL];
 #pragma unroll
             for (int q = 0; q < NPL; ++q) {
                 const int j = lane + 32 * q;
-                if (j < K) mpole[(size_t)bx[a] * K + j] = acc[a][q];
+                tq[q] = (j < K) ? __ldg(T + (size_t)kk * K + j) : 0.0;
+            }
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a) {
+                const double v = s_in[si][a][kk];
+#pragma unroll
+                for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
+            }
+        }
+    }
+    if (MODE == 1) {
+#pragma unroll
+        for (int a = 0; a < TR_PB; ++a) {
+            if (ch[a] < 0) continue;
+#pragma unroll
+            for (int q = 0; q < NPL; ++q) {
+                const int j = lane + 32 * q;
+                if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
+            }
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < TR_PB; ++a)
+#pragma unroll
+            for (int q = 0; q < NPL; ++q) {
+                const int j = lane + 32 * q;
+                if (j < K) s_part[s][a][j] = acc[a][q];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < TR_PB; ++a) {
+            if (bx[a] < 0) continue;
+            for (int d = threadIdx.x; d < K; d += blockDim.x) {
+                double v = 0.0;
+#pragma unroll
+                for (int o = 0; o < 8; ++o) v += s_part[o][a][d];
+                mpole[(size_t)bx[a] * K + d] = v;
             }
         }
     }
@@ -162,11 +165,9 @@ __global__ void __launch_bounds__(256) k_translate_tile(TreeView tv, int first, 
 
 template <int P>
 int launch_m2m(Handle& h, double* M) {
-    constexpr size_t smem = tt_smem<P>();
-    OGX_CUDA(cudaFuncSetAttribute(k_translate_tile<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int l = h.max_level - 1; l >= 0; --l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_tile<P, 0><<<(count + 8 * TT_PAR - 1) / (8 * TT_PAR), 256, smem, h.stream>>>(h.tv, first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+        const int first = h.nonleaf_off[l], count = h.nonleaf_off[l + 1] - first;
+        if (count > 0) { k_translate_oct<P, 0><<<(count + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf + first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -174,14 +175,12 @@ int launch_m2m(Handle& h, double* M) {
 template <int P>
 int launch_l2l(Handle& h, double* L, const double* Lown) {
     constexpr int K = (P + 1) * (P + 1);
-    constexpr size_t smem = tt_smem<P>();
-    OGX_CUDA(cudaFuncSetAttribute(k_translate_tile<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // root (no parent): its local is its own M2L/P2L part
     OGX_CUDA(cudaMemcpyAsync(L + (size_t)h.level_off[0] * K, Lown + (size_t)h.level_off[0] * K, sizeof(double) * K,
                              cudaMemcpyDeviceToDevice, h.stream));
     for (int l = 0; l < h.max_level; ++l) {
-        const int first = h.level_off[l], count = h.level_off[l + 1] - first;
-        if (count > 0) { k_translate_tile<P, 1><<<(count + 8 * TT_PAR - 1) / (8 * TT_PAR), 256, smem, h.stream>>>(h.tv, first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+        const int first = h.nonleaf_off[l], count = h.nonleaf_off[l + 1] - first;
+        if (count > 0) { k_translate_oct<P, 1><<<(count + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf + first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -467,7 +466,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(launch_l2l<P>(h, L, Lown));
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     const bool pot = d_pot != nullptr;
-    OGX_TRY((launch_far<P, float>(h, M, L, far, pot)));
+    OGX_TRY(launch_far32<P>(h, M, L, far, pot));
     const double G = h.prm.G;
     const float eps2 = (float)(h.prm.eps * h.prm.eps);
     if (pot) { mixed::k_leaf_near32<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }

@@ -75,6 +75,7 @@ enum Slot {
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
+    S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF,
     S_NUM_SLOTS
 };
 
@@ -180,6 +181,9 @@ struct Handle {
     int ntgt_pad = 0;                     // padded per-octant layout, 64 per tile
     const uint32_t* tgt_tile_key = nullptr;
     const uint32_t* tgt_tile_box = nullptr;
+    // non-leaf boxes, level-major (M2M / L2L parents); nonleaf_off[l] = first of level l
+    const int* d_nonleaf = nullptr;
+    std::vector<int32_t> nonleaf_off;
 };
 
 // ---- host-side operator tables (ogx_tables.cpp) -----------------------------

@@ -473,5 +473,188 @@ __global__ void __launch_bounds__(128) k_leaf_near32(TreeView tv, double G, floa
     }
 }
 
+// ---- leaf far field in FP32 (L2P + W-list M2P) ----------------------------------------
+// Coefficient records, one 8-float entry per (n, m >= 0), entry index n(n+1)/2 + m:
+//   {gx.re', gx.im', gy.re', gy.im', gz.re', gz.im', phi.re', phi.im'}
+// where the real-part weights are folded in (m = 0: (c.re, 0); m > 0: (2 c.re,
+// -2 c.im)) so that sum_nm Re(c_nm z_nm) = sum_e re' z.re + im' z.im, two 16-byte
+// loads feeding eight FMAs per harmonic.  The gradient coefficient sets are those
+// of fmm::localField / fmm::multipoleField (src3d/FmmExpansions3D.hpp:180-235):
+//   MODE 0, M2P source box: grad of degree P+1, phi of degree P (from M')
+//   MODE 1, L2P leaf:       grad of degree P-1, phi of degree P (from L')
+template <int P>
+struct FarRec32 {
+    static constexpr int NEH = (P + 2) * (P + 3) / 2;   // entries of an M2P record
+    static constexpr int NEG = (P + 1) * (P + 2) / 2;   // entries of an L2P record
+};
+
+template <int P, int MODE>
+__global__ void __launch_bounds__(128) k_far_rec32(TreeView tv, int count, const double* __restrict__ coef,
+                                                   float4* __restrict__ rec) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int NE = MODE == 0 ? FarRec32<P>::NEH : FarRec32<P>::NEG;
+    const int lane = threadIdx.x & 31;
+    const int k = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (k >= count) return;
+    const int b = (MODE == 0) ? k : tv.leafbox[k];
+    if (MODE == 0 && tv.x_off[b] == tv.x_off[b + 1]) return;   // never an M2P source
+    const double* c = coef + (size_t)b * K;
+    float4* o = rec + (size_t)k * 2 * NE;
+    for (int e = lane; e < NE; e += 32) {
+        int n = 0;
+        while ((n + 1) * (n + 2) / 2 <= e) ++n;
+        const int m = e - n * (n + 1) / 2;
+        const int dr = dof_re(n, m);
+        float gr[3] = {0.f, 0.f, 0.f}, gi[3] = {0.f, 0.f, 0.f};
+        float pr = 0.f, pi = 0.f;
+        if (MODE == 0) {
+            mpole_grad_dof(c, dr, gr);
+            if (m > 0) mpole_grad_dof(c, dr + 1, gi);
+        } else if (n < P) {
+            local_grad_dof(c, dr, gr);
+            if (m > 0) local_grad_dof(c, dr + 1, gi);
+        }
+        if (n <= P) {
+            pr = (float)c[dr];
+            if (m > 0) pi = (float)c[dr + 1];
+        }
+        const float wr = m == 0 ? 1.f : 2.f, wi = m == 0 ? 0.f : -2.f;
+        o[2 * e] = make_float4(wr * gr[0], wi * gi[0], wr * gr[1], wi * gi[1]);
+        o[2 * e + 1] = make_float4(wr * gr[2], wi * gi[2], wr * pr, wi * pi);
+    }
+}
+
+__device__ __forceinline__ void far_term(const float4* r, int e, float re, float im, float& ax, float& ay, float& az,
+                                         float& ph) {
+    const float4 c0 = r[2 * e], c1 = r[2 * e + 1];
+    ax = fmaf(c0.x, re, fmaf(c0.y, im, ax));
+    ay = fmaf(c0.z, re, fmaf(c0.w, im, ay));
+    az = fmaf(c1.x, re, fmaf(c1.y, im, az));
+    ph = fmaf(c1.z, re, fmaf(c1.w, im, ph));
+}
+
+// shared-memory records per warp: up to FAR_R M2P records (or the leaf's L2P record)
+constexpr int FAR_R = 4;
+template <int P>
+constexpr int far_warp_f4() { return FAR_R * 2 * FarRec32<P>::NEH; }
+template <int P>
+constexpr size_t far_smem_bytes() { return 4 * sizeof(float4) * (size_t)far_warp_f4<P>(); }
+
+// Warp per leaf, bodies in blocks of 64 (positions relative to the leaf centre
+// staged in FP64 shared memory).  L2P: lanes over bodies.  M2P: the (body,
+// W box) pairs of the block form a flat W-major task list; a round takes up to
+// 32 consecutive tasks spanning at most FAR_R W boxes, whose records the warp
+// first copies into shared memory with coalesced 16-byte loads, so a leaf of 17
+// bodies and 9 W boxes keeps every lane busy and the harmonic loop reads shared
+// memory only.  Each round's task results go through shared memory and every
+// body sums its own in task order (deterministic); totals accumulate in FP64.
+template <int P, bool POT>
+__global__ void __launch_bounds__(128, 6) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
+                                                       const float4* __restrict__ grec, double* __restrict__ far) {
+    constexpr int NEH = FarRec32<P>::NEH, NEG = FarRec32<P>::NEG;
+    extern __shared__ float4 s_far_dyn[];
+    __shared__ double s_pos[4][3][64];
+    __shared__ float4 s_res[4][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= tv.nleaf) return;
+    float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
+    const int b = tv.leafbox[lf];
+    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+    const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
+    const int64_t w0 = tv.w_off[lf];
+    const int nw = (int)(tv.w_off[lf + 1] - w0);
+    const float4* g = grec + (size_t)lf * 2 * NEG;
+    double* sx = s_pos[wid][0];
+    double* sy = s_pos[wid][1];
+    double* sz = s_pos[wid][2];
+    for (int jb = 0; jb < cnt; jb += 64) {
+        const int nbk = min(64, cnt - jb);
+        __syncwarp();
+        for (int j = lane; j < nbk; j += 32) {
+            const int i = f0 + jb + j;
+            sx[j] = tv.px[i] - cx;
+            sy[j] = tv.py[i] - cy;
+            sz[j] = tv.pz[i] - cz;
+        }
+        for (int i = lane; i < 2 * NEG; i += 32) srec[i] = __ldg(g + i);
+        __syncwarp();
+        double acc[2][4];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0;
+            const int j = lane + 32 * q;
+            if (j < nbk) {
+                const float ux = (float)(sx[j] * inv), uy = (float)(sy[j] * inv), uz = (float)(sz[j] * inv);
+                float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+                for_regular<P>(ux, uy, uz, [&](int n, int m, float re, float im) {
+                    far_term(srec, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
+                });
+                acc[q][0] = (double)ax * inv;
+                acc[q][1] = (double)ay * inv;
+                acc[q][2] = (double)az * inv;
+                acc[q][3] = (double)ph;
+            }
+        }
+        const int total = nbk * nw;
+        for (int b0 = 0; b0 < total;) {
+            const int wa = b0 / nbk;
+            const int end = min(total, min(b0 + 32, (wa + FAR_R) * nbk));
+            const int nrec = (end - 1) / nbk - wa + 1;
+            __syncwarp();
+            for (int i = lane; i < nrec * 2 * NEH; i += 32) {
+                const int r = i / (2 * NEH), off = i - r * (2 * NEH);
+                srec[i] = __ldg(hrec + (size_t)tv.w_idx[w0 + wa + r] * 2 * NEH + off);
+            }
+            __syncwarp();
+            const int t = b0 + lane;
+            float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (t < end) {
+                const int w = t / nbk, j = t - w * nbk;
+                const int c = tv.w_idx[w0 + w];
+                const double2 c01 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c);
+                const double2 c23 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c + 1);
+                const float winv = 1.0f / (2.0f * (float)c23.y);
+                const float ux = (float)(sx[j] + (cx - c01.x)) * winv;
+                const float uy = (float)(sy[j] + (cy - c01.y)) * winv;
+                const float uz = (float)(sz[j] + (cz - c23.x)) * winv;
+                const float4* hr = srec + (w - wa) * 2 * NEH;
+                float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+                for_singular<P + 1>(ux, uy, uz, [&](int n, int m, float re, float im) {
+                    far_term(hr, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
+                });
+                const float w2 = winv * winv;
+                res = make_float4(ax * w2, ay * w2, az * w2, POT ? ph * winv : 0.f);
+            }
+            s_res[wid][lane] = res;
+            __syncwarp();
+            const int bm = b0 % nbk;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int j = lane + 32 * q;
+                if (j < nbk) {
+                    int k = j - bm;
+                    if (k < 0) k += nbk;
+                    for (; b0 + k < end; k += nbk) {
+                        const float4 v = s_res[wid][k];
+                        acc[q][0] += v.x; acc[q][1] += v.y; acc[q][2] += v.z; acc[q][3] += v.w;
+                    }
+                }
+            }
+            b0 = end;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = lane + 32 * q;
+            if (j < nbk) {
+                double2* o = reinterpret_cast<double2*>(far + 4 * (size_t)(f0 + jb + j));
+                o[0] = make_double2(acc[q][0], acc[q][1]);
+                o[1] = make_double2(acc[q][2], acc[q][3]);
+            }
+        }
+    }
+}
+
 }  // namespace mixed
 }  // namespace ogx
