@@ -62,10 +62,10 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
     const size_t smem = mixed::far_smem_bytes<P>();
     if (pot) {
         OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mixed::k_leaf_far32<P, true><<<(tv.nleaf + 3) / 4, 128, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+        mixed::k_leaf_far32<P, true><<<(tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, 32 * mixed::FAR_WARPS, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     } else {
         OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mixed::k_leaf_far32<P, false><<<(tv.nleaf + 3) / 4, 128, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+        mixed::k_leaf_far32<P, false><<<(tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, 32 * mixed::FAR_WARPS, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     }
     return OGX_OK;
 }

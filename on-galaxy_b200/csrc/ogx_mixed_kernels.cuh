@@ -22,9 +22,12 @@
 //   * operands: A rows are gathered with cp.async into the canonical K-major
 //     no-swizzle layout (8-row x 16-byte core matrices); each T_o chunk is a
 //     pre-laid-out image copied by the TMA bulk engine (cp.async.bulk, no
-//     multicast); K is cut into chunks of 32 so 4 stages pipeline through
-//     mbarriers; one warp issues the MMAs (one lane), four warps produce the
-//     operands, drain the accumulators and write the result.
+//     multicast); K is cut into chunks of 32 so up to 4 stages pipeline through
+//     mbarriers;
+//   * warp specialisation: four warps gather the A rows (the colleague table
+//     of the tile is staged in shared memory and the next combination's source
+//     index is fetched one combination ahead), one lane issues the MMAs, and
+//     eight drain warps fold each combination into FP64 and write the result.
 // Output degree 0 (L_0^0, only needed for potentials) is excluded from N.
 // TMEM holds 2 x N FP32 + 2 x N FP64-halves columns, so the tensor-core path
 // serves p <= 10 (N <= 128); higher orders use the FP64 M2L kernel.
@@ -67,7 +70,14 @@ __host__ __device__ __forceinline__ int core_off(int row, int kk, int sbo) {
     return (row >> 3) * sbo + (kk >> 2) * 128 + (row & 7) * 16 + (kk & 3) * 4;
 }
 
-constexpr int TC_THREADS = 160;  // warps 0-3 producers + epilogue, warp 4 MMA issuer
+// Warp roles: warps 0-3 gather the A rows (thread r owns target row r), warp 4
+// issues the MMAs (one lane), warps 5..5+TC_DRAIN_WARPS-1 fold every combination's
+// FP32 result into the FP64 accumulator and write the tile's result.  A warp may
+// only touch the TMEM lane quarter (warp index mod 4), so the drain warps come in
+// groups of four, each group owning a slice of the output columns.
+constexpr int TC_PRODUCERS = 128;
+constexpr int TC_DRAIN_WARPS = 8;
+constexpr int TC_THREADS = TC_PRODUCERS + 32 + 32 * TC_DRAIN_WARPS;
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(
@@ -78,12 +88,12 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
 }
 __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// Add the FP32 combination result in D buffer `a` to the FP64 accumulator (this
-// warp's 32 lanes); `first` initialises the accumulator instead of adding.
+// Add the FP32 combination result in D buffer `a` (16-column groups g0..g1-1) to
+// the FP64 accumulator of this warp's 32 lanes; `first` initialises it instead.
 template <int NPAD, int ACC64>
-__device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first) {
+__device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first, int g0, int g1) {
 #pragma unroll 1
-    for (int c16 = 0; c16 < NPAD / 16; ++c16) {
+    for (int c16 = g0; c16 < g1; ++c16) {
         uint32_t v[16], lo[16], hi[16];
         sm100::tmem_ld16(tmem_lane + a * NPAD + c16 * 16, v);
         if (!first) {
@@ -111,27 +121,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
              double* __restrict__ lown, int* err) {
     using C = TcCfg<P>;
     static_assert(C::SUPPORTED, "tensor-core M2L serves p <= 10");
+    // gathers kept in flight per producer thread before its row is handed to the MMA
+    constexpr int LAG = C::STAGES >= 4 ? C::STAGES - 2 : 1;
+    constexpr int NG = C::NPAD / 16;
+    constexpr int NGRP = TC_DRAIN_WARPS / 4;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     __shared__ uint64_t afull[C::STAGES], bfull[C::STAGES], empty[C::STAGES], dfull[2], dempty[2], fin;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
-    __shared__ int s_t;
-    __shared__ int s_parent[128];
+    __shared__ int s_t, s_ncombo;
+    __shared__ int s_box[128];
+    __shared__ int s_Q[27][128];      // colleague slot D of each target's parent
     __shared__ uint32_t s_mask[6];
+    __shared__ int s_combo[189];      // present combinations: D | s << 5 | o << 8
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int base = blockIdx.x * 128;
     if (tid == 0) {
         s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
         s_abort = 0;
         for (int s = 0; s < C::STAGES; ++s) {
-            sm100::mbar_init(&afull[s], 128);
+            sm100::mbar_init(&afull[s], TC_PRODUCERS);
             sm100::mbar_init(&bfull[s], 1);
             sm100::mbar_init(&empty[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
             sm100::mbar_init(&dfull[a], 1);
-            sm100::mbar_init(&dempty[a], 128);
+            sm100::mbar_init(&dempty[a], 32 * TC_DRAIN_WARPS);
         }
         sm100::mbar_init(&fin, 1);
         sm100::fence_mbar_init();
@@ -142,45 +158,71 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (t < 0) return;
     const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
     if (warp == 4) sm100::tmem_alloc(&s_tmem, C::TMEM_COLS);
-    int myb = -1;
     if (tid < 128) {
         const uint32_t key = tgt_key[base + tid];
-        myb = (key == (uint32_t)t) ? (int)tgt_box[base + tid] : -1;
-        s_parent[tid] = (myb >= 0) ? tv.parent[myb] : -1;
+        const int myb = (key == (uint32_t)t) ? (int)tgt_box[base + tid] : -1;
+        s_box[tid] = myb;
+        const int par = (myb >= 0) ? tv.parent[myb] : -1;
+#pragma unroll 9
+        for (int D = 0; D < 27; ++D) s_Q[D][tid] = (par >= 0) ? tv.col[27 * par + D] : -1;
     }
     __syncthreads();
     // presence mask over the 189 (D, s) combinations of octant t
     if (tid < 128) {
-        const int par = s_parent[tid];
         int ci = 0;
         for (int D = 0; D < 27; ++D) {
-            const int Q = (par >= 0) ? tv.col[27 * par + D] : -1;
+            const int Q = s_Q[D][tid];
+            int ch[8];
+            if (Q >= 0) {
+                const int4 c0 = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Q));
+                const int4 c1 = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Q) + 1);
+                ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
+                ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
+            } else {
+#pragma unroll
+                for (int s = 0; s < 8; ++s) ch[s] = -1;
+            }
             const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+#pragma unroll
             for (int s = 0; s < 8; ++s) {
                 const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
                 if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
-                const bool has = (Q >= 0) && (tv.child[8 * Q + s] >= 0);
-                const unsigned bal = __ballot_sync(0xffffffffu, has);
+                const unsigned bal = __ballot_sync(0xffffffffu, ch[s] >= 0);
                 if (lane == 0 && bal) atomicOr(&s_mask[ci >> 5], 1u << (ci & 31));
                 ++ci;
             }
         }
     }
+    __syncthreads();
+    if (tid == 0) {
+        int n = 0, ci = 0;
+        for (int D = 0; D < 27; ++D) {
+            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+            for (int s = 0; s < 8; ++s) {
+                const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
+                if ((s_mask[ci >> 5] >> (ci & 31)) & 1u)
+                    s_combo[n++] = D | (s << 5) | (((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) << 8);
+                ++ci;
+            }
+        }
+        s_ncombo = n;
+    }
     sm100::tc_fence_before();
     __syncthreads();
     sm100::tc_fence_after();
     const uint32_t tmem = s_tmem;
+    const int nco = s_ncombo;
 
     if (warp == 4) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = sm100::idesc_tf32(C::M, C::NPAD);
-            int u = 0, cc = 0;
-            for (int ci = 0; ci < 189 && !s_abort; ++ci) {
-                if (!((s_mask[ci >> 5] >> (ci & 31)) & 1u)) continue;
-                const int a = cc & 1;
-                if (cc >= 2) {
-                    if (!sm100::mbar_wait(&dempty[a], ((cc >> 1) - 1) & 1, &s_abort)) {
+            int u = 0;
+            for (int k = 0; k < nco && !s_abort; ++k) {
+                const int a = k & 1;
+                if (k >= 2) {
+                    if (!sm100::mbar_wait(&dempty[a], ((k >> 1) - 1) & 1, &s_abort)) {
                         s_abort = 1;
                         atomicExch(err, 1);
                         break;
@@ -215,106 +257,109 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     sm100::mma_commit(&empty[s]);
                 }
                 sm100::mma_commit(&dfull[a]);
-                ++cc;
             }
             // completion of every MMA this thread issued (normal end and abort alike)
             sm100::mma_commit(&fin);
             if (!sm100::mbar_wait(&fin, 0, nullptr)) atomicExch(err, 1);
         }
         __syncwarp();
-    } else {
-        // ---------------- producers (thread tid owns target row tid) ----------------
+    } else if (warp < 4) {
+        // ---------------- producers: thread r gathers target row r ----------------
         const int r = tid;
-        const int par = s_parent[r];
-        const uint32_t tmem_lane = tmem + ((uint32_t)(warp * 32) << 16);
-        int u = 0, cc = 0, ci = 0;
+        int u = 0;
         bool bulk_pending[C::STAGES];
         uint32_t bulk_phase[C::STAGES];
         for (int s = 0; s < C::STAGES; ++s) bulk_pending[s] = false, bulk_phase[s] = 0;
-        auto drain = [&](int which) -> bool {
-            const int a = which & 1;
-            if (!sm100::mbar_wait(&dfull[a], (which >> 1) & 1, &s_abort)) {
-                s_abort = 1;
-                atomicExch(err, 1);
-                return false;
+        // source box of the next combination, fetched one combination ahead
+        int src_next = -1;
+        if (nco > 0) {
+            const int c0 = s_combo[0];
+            const int Q = s_Q[c0 & 31][r];
+            src_next = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((c0 >> 5) & 7)) : -1;
+        }
+        for (int k = 0; k < nco && !s_abort; ++k) {
+            const int code = s_combo[k];
+            const int src = src_next;
+            if (k + 1 < nco) {
+                const int c1 = s_combo[k + 1];
+                const int Q = s_Q[c1 & 31][r];
+                src_next = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((c1 >> 5) & 7)) : -1;
             }
-            sm100::tc_fence_after();
-            drain_combo<C::NPAD, C::ACC64>(tmem_lane, a, which == 0);
-            sm100::tc_fence_before();
-            sm100::mbar_arrive(&dempty[a]);
-            return true;
-        };
-        for (int D = 0; D < 27 && !s_abort; ++D) {
-            const int Q = (par >= 0) ? tv.col[27 * par + D] : -1;
-            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
-            for (int s8 = 0; s8 < 8 && !s_abort; ++s8) {
-                const int ox = 2 * Dx + (s8 & 1) - tx, oy = 2 * Dy + ((s8 >> 1) & 1) - ty, oz = 2 * Dz + ((s8 >> 2) & 1) - tz;
-                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
-                const int my_ci = ci++;
-                if (!((s_mask[my_ci >> 5] >> (my_ci & 31)) & 1u)) continue;
-                const int src = (Q >= 0) ? tv.child[8 * Q + s8] : -1;
-                const int o = (ox + 3) + 7 * (oy + 3) + 49 * (oz + 3);
-                for (int c = 0; c < C::NCH; ++c, ++u) {
-                    const int s = u % C::STAGES;
-                    if (u >= C::STAGES) {
-                        if (!sm100::mbar_wait(&empty[s], ((u / C::STAGES) - 1) & 1, &s_abort)) {
-                            s_abort = 1;
-                            atomicExch(err, 1);
-                            break;
-                        }
-                        bulk_pending[s] = false;
+            const int o = code >> 8;
+            for (int c = 0; c < C::NCH; ++c, ++u) {
+                const int s = u % C::STAGES;
+                if (u >= C::STAGES) {
+                    if (!sm100::mbar_wait(&empty[s], ((u / C::STAGES) - 1) & 1, &s_abort)) {
+                        s_abort = 1;
+                        atomicExch(err, 1);
+                        break;
                     }
-                    uint8_t* st = smem + (size_t)s * C::STAGE_BYTES;
-                    if (r == 0) {
-                        const uint8_t* bsrc = btab + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
-                        sm100::mbar_arrive_expect_tx(&bfull[s], 2 * C::B_BYTES);
-                        sm100::bulk_g2s(st + 2 * C::A_BYTES, bsrc, C::B_BYTES, &bfull[s]);
-                        sm100::bulk_g2s(st + 2 * C::A_BYTES + C::B_BYTES, bsrc + C::B_BYTES, C::B_BYTES, &bfull[s]);
-                        bulk_pending[s] = true;
-                        bulk_phase[s] = (u / C::STAGES) & 1;
+                    bulk_pending[s] = false;
+                }
+                uint8_t* st = smem + (size_t)s * C::STAGE_BYTES;
+                if (r == 0) {
+                    const uint8_t* bsrc = btab + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
+                    sm100::mbar_arrive_expect_tx(&bfull[s], 2 * C::B_BYTES);
+                    sm100::bulk_g2s(st + 2 * C::A_BYTES, bsrc, C::B_BYTES, &bfull[s]);
+                    sm100::bulk_g2s(st + 2 * C::A_BYTES + C::B_BYTES, bsrc + C::B_BYTES, C::B_BYTES, &bfull[s]);
+                    bulk_pending[s] = true;
+                    bulk_phase[s] = (u / C::STAGES) & 1;
+                }
+                const int k0 = c * C::CH * 8;
+                const int nq = min(2 * C::CH, (C::KPAD - k0) / 4);
+                if (src >= 0) {
+                    const float* gh = mhi + (size_t)src * C::KPAD + k0;
+                    const float* gl = mlo + (size_t)src * C::KPAD + k0;
+                    for (int q = 0; q < nq; ++q) {
+                        sm100::cp_async16(st + core_off(r, 4 * q, C::SBO), gh + 4 * q);
+                        sm100::cp_async16(st + C::A_BYTES + core_off(r, 4 * q, C::SBO), gl + 4 * q);
                     }
-                    const int k0 = c * C::CH * 8;
-                    const int nq = min(2 * C::CH, (C::KPAD - k0) / 4);
-                    if (src >= 0) {
-                        const float* gh = mhi + (size_t)src * C::KPAD + k0;
-                        const float* gl = mlo + (size_t)src * C::KPAD + k0;
-                        for (int q = 0; q < nq; ++q) {
-                            sm100::cp_async16(st + core_off(r, 4 * q, C::SBO), gh + 4 * q);
-                            sm100::cp_async16(st + C::A_BYTES + core_off(r, 4 * q, C::SBO), gl + 4 * q);
-                        }
-                    } else {
-                        for (int q = 0; q < nq; ++q) {
-                            *(float4*)(st + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
-                            *(float4*)(st + C::A_BYTES + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
-                        }
-                    }
-                    sm100::cp_async_commit();
-                    if (u >= 1) {
-                        sm100::cp_async_wait<1>();
-                        sm100::fence_proxy_async();
-                        sm100::mbar_arrive(&afull[(u - 1) % C::STAGES]);
+                } else {
+                    for (int q = 0; q < nq; ++q) {
+                        *(float4*)(st + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
+                        *(float4*)(st + C::A_BYTES + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
                     }
                 }
-                // every unit of combination cc is issued: fold combination cc-1 into FP64
-                if (cc >= 1 && !s_abort) drain(cc - 1);
-                ++cc;
+                sm100::cp_async_commit();
+                if (u >= LAG) {
+                    sm100::cp_async_wait<LAG>();
+                    sm100::fence_proxy_async();
+                    sm100::mbar_arrive(&afull[(u - LAG) % C::STAGES]);
+                }
             }
         }
         sm100::cp_async_wait<0>();
         sm100::fence_proxy_async();
-        if (u >= 1 && !s_abort) sm100::mbar_arrive(&afull[(u - 1) % C::STAGES]);
-        if (cc >= 1 && !s_abort) drain(cc - 1);
+        if (!s_abort)
+            for (int v = max(0, u - LAG); v < u; ++v) sm100::mbar_arrive(&afull[v % C::STAGES]);
         if (s_abort && r == 0) {
             // let this thread's bulk copies land before the CTA exits
             for (int s = 0; s < C::STAGES; ++s)
                 if (bulk_pending[s]) sm100::mbar_wait(&bfull[s], bulk_phase[s], nullptr);
         }
-        // ---------------- epilogue: FP64 accumulator -> L_own (row tid = target) ----------------
-        if (cc >= 1 && !s_abort) {
+    } else {
+        // ---------------- drain warps: FP32 combination -> FP64 accumulator -> L_own ----------------
+        const int quarter = warp & 3;                 // the TMEM lane quarter this warp may access
+        const int grp = (warp - 5) >> 2;              // column slice of this warp
+        const int g0 = grp * NG / NGRP, g1 = (grp + 1) * NG / NGRP;
+        const uint32_t tmem_lane = tmem + ((uint32_t)(quarter * 32) << 16);
+        for (int k = 0; k < nco && !s_abort; ++k) {
+            const int a = k & 1;
+            if (!sm100::mbar_wait(&dfull[a], (k >> 1) & 1, &s_abort)) {
+                s_abort = 1;
+                atomicExch(err, 1);
+                break;
+            }
             sm100::tc_fence_after();
+            drain_combo<C::NPAD, C::ACC64>(tmem_lane, a, k == 0, g0, g1);
+            sm100::tc_fence_before();
+            sm100::mbar_arrive(&dempty[a]);
+        }
+        if (nco >= 1 && !s_abort) {
+            const int myb = s_box[quarter * 32 + lane];
             const double inv = (myb >= 0) ? 1.0 / (2.0 * tv.center[4 * myb + 3]) : 0.0;
 #pragma unroll 1
-            for (int c16 = 0; c16 < C::NPAD / 16; ++c16) {
+            for (int c16 = g0; c16 < g1; ++c16) {
                 uint32_t lo[16], hi[16];
                 sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32, lo);
                 sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32 + 16, hi);
@@ -535,10 +580,13 @@ __device__ __forceinline__ void far_term(const float4* r, int e, float re, float
 
 // shared-memory records per warp: up to FAR_R M2P records (or the leaf's L2P record)
 constexpr int FAR_R = 4;
+// one warp per block: a block's resources return as soon as its leaf is done,
+// so leaves of very different cost do not hold idle warps resident
+constexpr int FAR_WARPS = 1;
 template <int P>
 constexpr int far_warp_f4() { return FAR_R * 2 * FarRec32<P>::NEH; }
 template <int P>
-constexpr size_t far_smem_bytes() { return 4 * sizeof(float4) * (size_t)far_warp_f4<P>(); }
+constexpr size_t far_smem_bytes() { return FAR_WARPS * sizeof(float4) * (size_t)far_warp_f4<P>(); }
 
 // Warp per leaf, bodies in blocks of 64 (positions relative to the leaf centre
 // staged in FP64 shared memory).  L2P: lanes over bodies.  M2P: the (body,
@@ -549,14 +597,14 @@ constexpr size_t far_smem_bytes() { return 4 * sizeof(float4) * (size_t)far_warp
 // memory only.  Each round's task results go through shared memory and every
 // body sums its own in task order (deterministic); totals accumulate in FP64.
 template <int P, bool POT>
-__global__ void __launch_bounds__(128, 6) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
+__global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
                                                        const float4* __restrict__ grec, double* __restrict__ far) {
     constexpr int NEH = FarRec32<P>::NEH, NEG = FarRec32<P>::NEG;
     extern __shared__ float4 s_far_dyn[];
-    __shared__ double s_pos[4][3][64];
-    __shared__ float4 s_res[4][32];
+    __shared__ double s_pos[FAR_WARPS][3][64];
+    __shared__ float4 s_res[FAR_WARPS][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int lf = blockIdx.x * 4 + wid;
+    const int lf = blockIdx.x * FAR_WARPS + wid;
     if (lf >= tv.nleaf) return;
     float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
     const int b = tv.leafbox[lf];
