@@ -394,7 +394,7 @@ int ensure_mixed_tables(Handle& h) {
                     const double x = T[(size_t)(jr + 1) * K + k];
                     const float vh = rna_tf32((float)x);
                     const float vl = rna_tf32((float)(x - (double)vh));
-                    const int off = mixed::core_off(jr, kk, C::SBO);
+                    const int off = mixed::tile_off(jr, kk);
                     std::memcpy(hi + off, &vh, 4);
                     std::memcpy(lo + off, &vl, 4);
                 }

@@ -54,7 +54,7 @@ struct TcCfg {
     static constexpr int N = K - 1;           // output dofs 1..K-1
     static constexpr int NPAD = (N + 15) / 16 * 16;
     static constexpr int M = 128;
-    static constexpr int SBO = CH * 2 * 128;  // bytes between 8-row groups
+    static constexpr int SBO = 1024;          // bytes between 8-row groups (one swizzle atom)
     static constexpr int A_BYTES = (M / 8) * SBO;
     static constexpr int B_BYTES = (NPAD / 8) * SBO;
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -63,11 +63,16 @@ struct TcCfg {
     static constexpr int ACC64 = 2 * NPAD;    // first column of the FP64 accumulator
     static constexpr int TMEM_COLS = 512;
     static constexpr bool SUPPORTED = 4 * NPAD <= 512 && STAGES >= 2;
+    static_assert(CH * 8 * 4 == 128, "a chunk row must fill exactly one 128-byte swizzle line");
 };
 
-// byte offset of element (row, kk) inside one operand stage (kk < CH*8)
-__host__ __device__ __forceinline__ int core_off(int row, int kk, int sbo) {
-    return (row >> 3) * sbo + (kk >> 2) * 128 + (row & 7) * 16 + (kk & 3) * 4;
+// Byte offset of element (row, kk), kk < 32, inside one operand of a stage, in the
+// K-major 128-byte-swizzle layout: each row's 32 tf32 of the chunk fill one
+// 128-byte line, 8 rows form a 1024-byte atom, and 16-byte piece j of row r sits
+// at piece position j ^ (r mod 8) so the tensor core reads the 8 rows of an atom
+// from different banks.  Operand bases are 1024-byte aligned.
+__host__ __device__ __forceinline__ int tile_off(int row, int kk) {
+    return (row >> 3) * 1024 + (row & 7) * 128 + ((((kk >> 2) ^ row) & 7) << 4) + (kk & 3) * 4;
 }
 
 // Warp roles: warps 0-3 gather the A rows (thread r owns target row r), warp 4
@@ -218,6 +223,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = sm100::idesc_tf32(C::M, C::NPAD);
+            // descriptors differ only in their 14-bit start-address field (bytes >> 4):
+            // build stage 0's once and add the stage / K-step / operand offsets
+            const uint64_t desc0 = sm100::smem_desc_sw128(sm100::smem_u32(smem), C::SBO);
+            constexpr uint32_t D_LO = C::A_BYTES >> 4, D_BHI = (2 * C::A_BYTES) >> 4,
+                               D_BLO = (2 * C::A_BYTES + C::B_BYTES) >> 4, D_STAGE = C::STAGE_BYTES >> 4;
             int u = 0;
             for (int k = 0; k < nco && !s_abort; ++k) {
                 const int a = k & 1;
@@ -240,19 +250,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     sm100::tc_fence_after();
-                    const uint32_t st = sm100::smem_u32(smem + (size_t)s * C::STAGE_BYTES);
-                    const uint32_t a_hi = st, a_lo = st + C::A_BYTES, b_hi = st + 2 * C::A_BYTES,
-                                   b_lo = b_hi + C::B_BYTES;
+                    const uint64_t ds = desc0 + (uint64_t)(s * D_STAGE);
                     const int nks = min(C::CH, C::NKS - c * C::CH);
-                    for (int ks = 0; ks < nks; ++ks) {
-                        const uint32_t ko = ks * 256;
-                        sm100::mma_tf32(dcol, sm100::smem_desc(a_hi + ko, 128, C::SBO), sm100::smem_desc(b_hi + ko, 128, C::SBO),
-                                        idesc, accum);
-                        accum = 1;
-                        sm100::mma_tf32(dcol, sm100::smem_desc(a_hi + ko, 128, C::SBO), sm100::smem_desc(b_lo + ko, 128, C::SBO),
-                                        idesc, 1);
-                        sm100::mma_tf32(dcol, sm100::smem_desc(a_lo + ko, 128, C::SBO), sm100::smem_desc(b_hi + ko, 128, C::SBO),
-                                        idesc, 1);
+#pragma unroll
+                    for (int ks = 0; ks < C::CH; ++ks) {
+                        if (ks < nks) {
+                            const uint64_t dk = ds + (uint64_t)(ks * 2);    // 32 bytes per K-step inside the line
+                            sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc, accum);
+                            accum = 1;
+                            sm100::mma_tf32(dcol, dk, dk + D_BLO, idesc, 1);
+                            sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);
+                        }
                     }
                     sm100::mma_commit(&empty[s]);
                 }
@@ -277,7 +285,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int Q = s_Q[c0 & 31][r];
             src_next = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((c0 >> 5) & 7)) : -1;
         }
-        for (int k = 0; k < nco && !s_abort; ++k) {
+        // exits are warp-uniform: the row copies below shuffle across the warp
+        for (int k = 0; k < nco && !__any_sync(0xffffffffu, s_abort != 0); ++k) {
             const int code = s_combo[k];
             const int src = src_next;
             if (k + 1 < nco) {
@@ -289,7 +298,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int c = 0; c < C::NCH; ++c, ++u) {
                 const int s = u % C::STAGES;
                 if (u >= C::STAGES) {
-                    if (!sm100::mbar_wait(&empty[s], ((u / C::STAGES) - 1) & 1, &s_abort)) {
+                    const bool ok = sm100::mbar_wait(&empty[s], ((u / C::STAGES) - 1) & 1, &s_abort);
+                    if (!__all_sync(0xffffffffu, ok)) {
                         s_abort = 1;
                         atomicExch(err, 1);
                         break;
@@ -305,19 +315,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     bulk_pending[s] = true;
                     bulk_phase[s] = (u / C::STAGES) & 1;
                 }
+                // the warp copies its 32 rows cooperatively: one instruction moves
+                // 16-byte pieces q0..q0+3 of 8 rows, so each source row is read in
+                // whole 64-byte runs and a quarter-warp fills 8 consecutive slots
                 const int k0 = c * C::CH * 8;
                 const int nq = min(2 * C::CH, (C::KPAD - k0) / 4);
-                if (src >= 0) {
-                    const float* gh = mhi + (size_t)src * C::KPAD + k0;
-                    const float* gl = mlo + (size_t)src * C::KPAD + k0;
-                    for (int q = 0; q < nq; ++q) {
-                        sm100::cp_async16(st + core_off(r, 4 * q, C::SBO), gh + 4 * q);
-                        sm100::cp_async16(st + C::A_BYTES + core_off(r, 4 * q, C::SBO), gl + 4 * q);
-                    }
-                } else {
-                    for (int q = 0; q < nq; ++q) {
-                        *(float4*)(st + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
-                        *(float4*)(st + C::A_BYTES + core_off(r, 4 * q, C::SBO)) = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int rl = 8 * (i >> 2) + (lane & 7);         // row within the warp
+                    const int part = (i >> 1) & 1;                    // 0: hi, 1: lo
+                    const int q = (i & 1) * 4 + (lane >> 3);          // 16-byte piece of the chunk
+                    const int rs = __shfl_sync(0xffffffffu, src, rl);
+                    if (q < nq) {
+                        const float* g = (part ? mlo : mhi) + (size_t)max(rs, 0) * C::KPAD + k0 + 4 * q;
+                        sm100::cp_async16_zfill(st + part * C::A_BYTES + tile_off(32 * warp + rl, 4 * q), g,
+                                                rs >= 0 ? 16u : 0u);
                     }
                 }
                 sm100::cp_async_commit();

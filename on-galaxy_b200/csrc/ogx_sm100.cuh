@@ -46,6 +46,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
 }
+// same, reading `bytes_valid` (0 or 16) bytes and zero-filling the rest
+__device__ __forceinline__ void cp_async16_zfill(void* sdst, const void* gsrc, uint32_t bytes_valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes_valid)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -81,6 +86,19 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
     d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
     return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
+}
+// Same, 128-byte swizzle (layout type 2): rows of 128 bytes, 8-row atoms of 1024
+// bytes `sbo` apart; the leading byte offset is unused for this layout (field 1).
+// The start address may advance inside the 128-byte line (K steps); the swizzle
+// is applied to absolute address bits, so the operand base must be 1024-aligned.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+    return d;
 }
 // Instruction descriptor: kind::tf32, D f32, A/B tf32, both K-major, dense.
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
