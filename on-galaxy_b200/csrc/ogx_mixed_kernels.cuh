@@ -29,8 +29,11 @@
 //     index is fetched one combination ahead), one lane issues the MMAs, and
 //     eight drain warps fold each combination into FP64 and write the result.
 // Output degree 0 (L_0^0, only needed for potentials) is excluded from N.
-// TMEM holds 2 x N FP32 + 2 x N FP64-halves columns, so the tensor-core path
-// serves p <= 10 (N <= 128); higher orders use the FP64 M2L kernel.
+// An MMA of N <= ~160 columns costs about the same time, so for p <= 8 the
+// operator's hi and lo images form one N = 2 N operand: A_hi x [B_hi | B_lo] and
+// A_lo x B_hi are two MMAs per K step (three otherwise).  TMEM holds two FP32
+// buffers (2 x 2N or 2 x N columns) + 2 x N FP64-halves columns, so the
+// tensor-core path serves p <= 10 (N <= 128); higher orders use the FP64 M2L kernel.
 //
 // Near field in FP32 on leaf-centred double-float coordinates (hi + lo FP32
 // relative to the target leaf centre, shift in FP64), r^-1 from rsqrt plus one
@@ -60,7 +63,13 @@ struct TcCfg {
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int STAGES = (220 * 1024 / STAGE_BYTES) >= 4 ? 4 : (220 * 1024 / STAGE_BYTES);
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024;
-    static constexpr int ACC64 = 2 * NPAD;    // first column of the FP64 accumulator
+    // Paired form (p <= 8): B_hi and B_lo are adjacent rows of one N = 2 NPAD operand,
+    // so A_hi x [B_hi | B_lo] is one MMA and A_lo x B_hi a second one (two MMAs per
+    // K-step instead of three; an MMA costs about the same time up to N ~ 160).
+    // A combination buffer then holds [hh + lh | hl], summed when drained.
+    static constexpr bool PAIR = 6 * NPAD <= 512;
+    static constexpr int DBUF = PAIR ? 2 * NPAD : NPAD;  // TMEM columns of one FP32 buffer
+    static constexpr int ACC64 = 2 * DBUF;    // first column of the FP64 accumulator
     static constexpr int TMEM_COLS = 512;
     static constexpr bool SUPPORTED = 4 * NPAD <= 512 && STAGES >= 2;
     static_assert(CH * 8 * 4 == 128, "a chunk row must fill exactly one 128-byte swizzle line");
@@ -95,12 +104,14 @@ __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.
 
 // Add the FP32 combination result in D buffer `a` (16-column groups g0..g1-1) to
 // the FP64 accumulator of this warp's 32 lanes; `first` initialises it instead.
-template <int NPAD, int ACC64>
+// PAIR: the buffer holds two partial products NPAD columns apart.
+template <int NPAD, int DBUF, int ACC64, bool PAIR>
 __device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first, int g0, int g1) {
 #pragma unroll 1
     for (int c16 = g0; c16 < g1; ++c16) {
-        uint32_t v[16], lo[16], hi[16];
-        sm100::tmem_ld16(tmem_lane + a * NPAD + c16 * 16, v);
+        uint32_t v[16], w[16], lo[16], hi[16];
+        sm100::tmem_ld16(tmem_lane + a * DBUF + c16 * 16, v);
+        if (PAIR) sm100::tmem_ld16(tmem_lane + a * DBUF + NPAD + c16 * 16, w);
         if (!first) {
             sm100::tmem_ld16(tmem_lane + ACC64 + c16 * 32, lo);
             sm100::tmem_ld16(tmem_lane + ACC64 + c16 * 32 + 16, hi);
@@ -109,6 +120,7 @@ __device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool firs
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             double s = (double)__uint_as_float(v[k]);
+            if (PAIR) s += (double)__uint_as_float(w[k]);
             if (!first) s += __hiloint2double((int)hi[k], (int)lo[k]);
             lo[k] = (uint32_t)__double2loint(s);
             hi[k] = (uint32_t)__double2hiint(s);
@@ -223,6 +235,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = sm100::idesc_tf32(C::M, C::NPAD);
+            constexpr uint32_t idesc2 = sm100::idesc_tf32(C::M, 2 * C::NPAD);
             // descriptors differ only in their 14-bit start-address field (bytes >> 4):
             // build stage 0's once and add the stage / K-step / operand offsets
             const uint64_t desc0 = sm100::smem_desc_sw128(sm100::smem_u32(smem), C::SBO);
@@ -239,7 +252,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     sm100::tc_fence_after();
                 }
-                const uint32_t dcol = tmem + a * C::NPAD;
+                const uint32_t dcol = tmem + a * C::DBUF;
                 uint32_t accum = 0;
                 for (int c = 0; c < C::NCH && !s_abort; ++c, ++u) {
                     const int s = u % C::STAGES;
@@ -256,10 +269,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     for (int ks = 0; ks < C::CH; ++ks) {
                         if (ks < nks) {
                             const uint64_t dk = ds + (uint64_t)(ks * 2);    // 32 bytes per K-step inside the line
-                            sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc, accum);
-                            accum = 1;
-                            sm100::mma_tf32(dcol, dk, dk + D_BLO, idesc, 1);
-                            sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);
+                            if constexpr (C::PAIR) {
+                                sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc2, accum);      // A_hi x [B_hi | B_lo]
+                                accum = 1;
+                                sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);    // A_lo x B_hi
+                            } else {
+                                sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc, accum);
+                                accum = 1;
+                                sm100::mma_tf32(dcol, dk, dk + D_BLO, idesc, 1);
+                                sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);
+                            }
                         }
                     }
                     sm100::mma_commit(&empty[s]);
@@ -363,7 +382,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             sm100::tc_fence_after();
-            drain_combo<C::NPAD, C::ACC64>(tmem_lane, a, k == 0, g0, g1);
+            drain_combo<C::NPAD, C::DBUF, C::ACC64, C::PAIR>(tmem_lane, a, k == 0, g0, g1);
             sm100::tc_fence_before();
             sm100::mbar_arrive(&dempty[a]);
         }
