@@ -469,8 +469,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(launch_far32<P>(h, M, L, far, pot));
     const double G = h.prm.G;
     const float eps2 = (float)(h.prm.eps * h.prm.eps);
-    if (pot) { mixed::k_leaf_near32<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
-    else { mixed::k_leaf_near32<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
+    if (pot) { mixed::k_leaf_near32<true><<<tv.nleaf, 32, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
+    else { mixed::k_leaf_near32<false><<<tv.nleaf, 32, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[7], st));
     OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaGetLastError());

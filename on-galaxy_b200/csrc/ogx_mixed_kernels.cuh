@@ -19,11 +19,10 @@
 //     fresh FP32 accumulator (two ping-pong buffers in TMEM) that the epilogue
 //     warps drain into an FP64 accumulator also kept in TMEM (two 32-bit
 //     columns per value) while the MMA warp proceeds with the next combination;
-//   * operands: A rows are gathered with cp.async into the canonical K-major
-//     no-swizzle layout (8-row x 16-byte core matrices); each T_o chunk is a
-//     pre-laid-out image copied by the TMA bulk engine (cp.async.bulk, no
-//     multicast); K is cut into chunks of 32 so up to 4 stages pipeline through
-//     mbarriers;
+//   * operands: K is cut into chunks of 32 tf32 (one 128-byte line per row) in
+//     the K-major 128-byte-swizzle layout; A rows are gathered with cp.async,
+//     each T_o chunk is a pre-laid-out image copied by the TMA bulk engine
+//     (cp.async.bulk, no multicast); up to 4 stages pipeline through mbarriers;
 //   * warp specialisation: four warps gather the A rows (the colleague table
 //     of the tile is staged in shared memory and the next combination's source
 //     index is fetched one combination ahead), one lane issues the MMAs, and
@@ -471,12 +470,13 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 
 constexpr int NEAR_STAGE = 64;
 
+// softened pair sum over staged sources q = q0, q0 + dq, ... < n
 template <bool SELF, bool POT>
-__device__ __forceinline__ void p2p_block(const float4* __restrict__ shi, const float4* __restrict__ slo, int n, int self_q,
-                                          float thx, float thy, float thz, float tlx, float tly, float tlz, float eps2,
-                                          float& ax, float& ay, float& az, float& ph) {
+__device__ __forceinline__ void p2p_block(const float4* __restrict__ shi, const float4* __restrict__ slo, int q0, int dq, int n,
+                                          int self_q, float thx, float thy, float thz, float tlx, float tly, float tlz,
+                                          float eps2, float& ax, float& ay, float& az, float& ph) {
 #pragma unroll 4
-    for (int q = 0; q < n; ++q) {
+    for (int q = q0; q < n; q += dq) {
         const float4 h = shi[q];
         const float4 l = slo[q];
         const float dx = (h.x - thx) + (l.x - tlx);
@@ -497,19 +497,33 @@ __device__ __forceinline__ void p2p_block(const float4* __restrict__ shi, const 
     }
 }
 
+__device__ __forceinline__ double group_sum(double v, int tpg) {
+    for (int off = tpg; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Warp per leaf (one warp per block, so a block's resources return as soon as
+// its leaf is done).  A leaf of cnt <= 32 bodies splits the warp into G groups
+// of tpg = next power of two >= cnt lanes: lane (g, t) owns target body t and
+// takes every G-th source of each staged block, so small leaves keep most lanes
+// busy; the groups' partial sums (compensated per U entry) are combined in FP64
+// with shuffles.  Larger leaves run 32 targets at a time with G = 1.
 template <bool POT>
-__global__ void __launch_bounds__(128) k_leaf_near32(TreeView tv, double G, float eps2, const double* __restrict__ far,
-                                                     double* __restrict__ acc, double* __restrict__ pot) {
-    __shared__ float4 s_hi[4][NEAR_STAGE], s_lo[4][NEAR_STAGE];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int lf = blockIdx.x * 4 + wid;
+__global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, double G, float eps2, const double* __restrict__ far,
+                                                    double* __restrict__ acc, double* __restrict__ pot) {
+    __shared__ float4 s_hi[NEAR_STAGE], s_lo[NEAR_STAGE];
+    const int lane = threadIdx.x & 31;
+    const int lf = blockIdx.x;
     if (lf >= tv.nleaf) return;
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     const double bcx = tv.center[4 * b], bcy = tv.center[4 * b + 1], bcz = tv.center[4 * b + 2];
     const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
-    for (int j0 = 0; j0 < cnt; j0 += 32) {
-        const int jj = j0 + lane;
+    int tpg = 1;
+    while (tpg < min(cnt, 32)) tpg <<= 1;
+    const int ngrp = 32 / tpg, grp = lane / tpg, tl = lane & (tpg - 1);
+    for (int j0 = 0; j0 < cnt; j0 += tpg) {
+        const int jj = j0 + tl;
         const bool act = jj < cnt;
         const int i = f0 + (act ? jj : 0);
         const double ddx = tv.px[i] - bcx, ddy = tv.py[i] - bcy, ddz = tv.pz[i] - bcz;
@@ -527,24 +541,28 @@ __global__ void __launch_bounds__(128) k_leaf_near32(TreeView tv, double G, floa
                     const int j = s0 + k0 + q;
                     const double ex = tv.px[j] - bcx, ey = tv.py[j] - bcy, ez = tv.pz[j] - bcz;
                     const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
-                    s_hi[wid][q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
-                    s_lo[wid][q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+                    s_hi[q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
+                    s_lo[q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
                 }
                 __syncwarp();
                 if (c == b)
-                    p2p_block<true, POT>(s_hi[wid], s_lo[wid], n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+                    p2p_block<true, POT>(s_hi, s_lo, grp, ngrp, n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
                 else
-                    p2p_block<false, POT>(s_hi[wid], s_lo[wid], n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+                    p2p_block<false, POT>(s_hi, s_lo, grp, ngrp, n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
             }
             kahan_add(sx, cx, ax); kahan_add(sy, cy, ay); kahan_add(sz, cz, az);
             if (POT) kahan_add(sp, cp, ph);
         }
-        if (act) {
+        const double nx = group_sum((double)sx - (double)cx, tpg);
+        const double ny = group_sum((double)sy - (double)cy, tpg);
+        const double nz = group_sum((double)sz - (double)cz, tpg);
+        const double np = POT ? group_sum((double)sp - (double)cp, tpg) : 0.0;
+        if (act && grp == 0) {
             const int o = tv.perm[i];
-            acc[3 * (size_t)o] = G * (far[4 * (size_t)i] + ((double)sx - (double)cx));
-            acc[3 * (size_t)o + 1] = G * (far[4 * (size_t)i + 1] + ((double)sy - (double)cy));
-            acc[3 * (size_t)o + 2] = G * (far[4 * (size_t)i + 2] + ((double)sz - (double)cz));
-            if (POT) pot[o] = -G * (far[4 * (size_t)i + 3] + ((double)sp - (double)cp));
+            acc[3 * (size_t)o] = G * (far[4 * (size_t)i] + nx);
+            acc[3 * (size_t)o + 1] = G * (far[4 * (size_t)i + 1] + ny);
+            acc[3 * (size_t)o + 2] = G * (far[4 * (size_t)i + 2] + nz);
+            if (POT) pot[o] = -G * (far[4 * (size_t)i + 3] + np);
         }
     }
 }
