@@ -59,13 +59,25 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
     OGX_TRY(arena_get(h.ws, S_EVAL_G, (size_t)tv.nleaf * 2 * R::NEG, &grec));
     mixed::k_far_rec32<P, 0><<<(tv.nb + 3) / 4, 128, 0, st>>>(tv, tv.nb, M, hrec); ++h.launches;
     mixed::k_far_rec32<P, 1><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, tv.nleaf, L, grec); ++h.launches;
+    // heavy leaves: list, then one CTA of FAR_HW warps per leaf
+    int* heavy;
+    OGX_TRY(arena_get(h.ws, S_FAR_HEAVY, (size_t)tv.nleaf + 2, &heavy));
+    int* ctr = heavy + tv.nleaf;
+    OGX_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(int), st));
+    mixed::k_far_heavy_list<<<(tv.nleaf + 255) / 256, 256, 0, st>>>(tv, heavy, ctr); ++h.launches;
+    const size_t hsmem = mixed::far_heavy_smem_bytes<P>();
     const size_t smem = mixed::far_smem_bytes<P>();
+    const int lgrid = (tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, lblock = 32 * mixed::FAR_WARPS;
     if (pot) {
+        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32_heavy<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        mixed::k_leaf_far32_heavy<P, true><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
         OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mixed::k_leaf_far32<P, true><<<(tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, 32 * mixed::FAR_WARPS, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+        mixed::k_leaf_far32<P, true><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     } else {
+        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32_heavy<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        mixed::k_leaf_far32_heavy<P, false><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
         OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        mixed::k_leaf_far32<P, false><<<(tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, 32 * mixed::FAR_WARPS, smem, st>>>(tv, hrec, grec, far); ++h.launches;
+        mixed::k_leaf_far32<P, false><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     }
     return OGX_OK;
 }

@@ -75,7 +75,7 @@ enum Slot {
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
-    S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF,
+    S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_FAR_HEAVY,
     S_NUM_SLOTS
 };
 

@@ -637,31 +637,123 @@ constexpr int far_warp_f4() { return FAR_R * 2 * FarRec32<P>::NEH; }
 template <int P>
 constexpr size_t far_smem_bytes() { return FAR_WARPS * sizeof(float4) * (size_t)far_warp_f4<P>(); }
 
-// Warp per leaf, bodies in blocks of 64 (positions relative to the leaf centre
-// staged in FP64 shared memory).  L2P: lanes over bodies.  M2P: the (body,
-// W box) pairs of the block form a flat W-major task list; a round takes up to
-// 32 consecutive tasks spanning at most FAR_R W boxes, whose records the warp
-// first copies into shared memory with coalesced 16-byte loads, so a leaf of 17
-// bodies and 9 W boxes keeps every lane busy and the harmonic loop reads shared
-// memory only.  Each round's task results go through shared memory and every
-// body sums its own in task order (deterministic); totals accumulate in FP64.
+// Leaves with more M2P tasks (bodies x W boxes) than this are handled by a CTA
+// of FAR_HW warps instead of a single warp (k_leaf_far32_heavy), so one leaf
+// with a long W list does not decide the kernel's length.
+constexpr int FAR_HEAVY = 1024;
+constexpr int FAR_HW = 8;
+
+// end of the M2P round that starts at task b0: at most 32 tasks spanning at most
+// FAR_R W boxes
+__device__ __forceinline__ int far_round_end(int b0, int nbk, int total) {
+    return min(total, min(b0 + 32, (b0 / nbk + FAR_R) * nbk));
+}
+
+// L2P of body block (nbk bodies staged in sx/sy/sz relative to the leaf centre):
+// lane owns bodies lane and lane + 32
+template <int P>
+__device__ __forceinline__ void far_l2p(const float4* __restrict__ g, int nbk, const double* sx, const double* sy,
+                                        const double* sz, double inv, float4* srec, int lane, double (&acc)[2][4]) {
+    constexpr int NEG = FarRec32<P>::NEG;
+    __syncwarp();
+    for (int i = lane; i < 2 * NEG; i += 32) srec[i] = __ldg(g + i);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        if (j < nbk) {
+            const float ux = (float)(sx[j] * inv), uy = (float)(sy[j] * inv), uz = (float)(sz[j] * inv);
+            float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+            for_regular<P>(ux, uy, uz, [&](int n, int m, float re, float im) {
+                far_term(srec, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
+            });
+            acc[q][0] += (double)ax * inv;
+            acc[q][1] += (double)ay * inv;
+            acc[q][2] += (double)az * inv;
+            acc[q][3] += (double)ph;
+        }
+    }
+}
+
+// One M2P round, tasks [b0, end) of the body block: the W records the round
+// needs go to shared memory first (coalesced 16-byte loads), then lane t of the
+// round evaluates task b0 + t; every body sums its own task results in task
+// order into acc (FP64).
+template <int P, bool POT>
+__device__ __forceinline__ void far_m2p_round(const TreeView& tv, const float4* __restrict__ hrec, int64_t w0, int nbk,
+                                              int b0, int end, const double* sx, const double* sy, const double* sz,
+                                              double cx, double cy, double cz, float4* srec, float4* sres, int lane,
+                                              double (&acc)[2][4]) {
+    constexpr int NEH = FarRec32<P>::NEH;
+    const int wa = b0 / nbk;
+    const int nrec = (end - 1) / nbk - wa + 1;
+    __syncwarp();
+    for (int i = lane; i < nrec * 2 * NEH; i += 32) {
+        const int r = i / (2 * NEH), off = i - r * (2 * NEH);
+        srec[i] = __ldg(hrec + (size_t)tv.w_idx[w0 + wa + r] * 2 * NEH + off);
+    }
+    __syncwarp();
+    const int t = b0 + lane;
+    float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t < end) {
+        const int w = t / nbk, j = t - w * nbk;
+        const int c = tv.w_idx[w0 + w];
+        const double2 c01 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c);
+        const double2 c23 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c + 1);
+        const float winv = 1.0f / (2.0f * (float)c23.y);
+        const float ux = (float)(sx[j] + (cx - c01.x)) * winv;
+        const float uy = (float)(sy[j] + (cy - c01.y)) * winv;
+        const float uz = (float)(sz[j] + (cz - c23.x)) * winv;
+        const float4* hr = srec + (w - wa) * 2 * NEH;
+        float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+        for_singular<P + 1>(ux, uy, uz, [&](int n, int m, float re, float im) {
+            far_term(hr, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
+        });
+        const float w2 = winv * winv;
+        res = make_float4(ax * w2, ay * w2, az * w2, POT ? ph * winv : 0.f);
+    }
+    sres[lane] = res;
+    __syncwarp();
+    const int bm = b0 % nbk;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int j = lane + 32 * q;
+        if (j < nbk) {
+            int k = j - bm;
+            if (k < 0) k += nbk;
+            for (; b0 + k < end; k += nbk) {
+                const float4 v = sres[k];
+                acc[q][0] += v.x; acc[q][1] += v.y; acc[q][2] += v.z; acc[q][3] += v.w;
+            }
+        }
+    }
+}
+
+// Warp per leaf (one warp per block, so a block's resources return as soon as
+// its leaf is done), bodies in blocks of 64 with positions relative to the leaf
+// centre staged in FP64 shared memory.  L2P: lanes over bodies.  M2P: the
+// (body, W box) pairs of the block form a flat W-major task list taken 32 at a
+// time (far_m2p_round), so a leaf of 17 bodies and 9 W boxes keeps every lane
+// busy.  Leaves with more than FAR_HEAVY tasks are left to k_leaf_far32_heavy.
 template <int P, bool POT>
 __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
-                                                       const float4* __restrict__ grec, double* __restrict__ far) {
-    constexpr int NEH = FarRec32<P>::NEH, NEG = FarRec32<P>::NEG;
+                                                                             const float4* __restrict__ grec,
+                                                                             double* __restrict__ far) {
+    constexpr int NEG = FarRec32<P>::NEG;
     extern __shared__ float4 s_far_dyn[];
     __shared__ double s_pos[FAR_WARPS][3][64];
     __shared__ float4 s_res[FAR_WARPS][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * FAR_WARPS + wid;
     if (lf >= tv.nleaf) return;
-    float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
-    const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
     const int64_t w0 = tv.w_off[lf];
     const int nw = (int)(tv.w_off[lf + 1] - w0);
+    if ((int64_t)cnt * nw > FAR_HEAVY) return;
+    float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
+    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+    const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
     const float4* g = grec + (size_t)lf * 2 * NEG;
     double* sx = s_pos[wid][0];
     double* sy = s_pos[wid][1];
@@ -675,70 +767,12 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(T
             sy[j] = tv.py[i] - cy;
             sz[j] = tv.pz[i] - cz;
         }
-        for (int i = lane; i < 2 * NEG; i += 32) srec[i] = __ldg(g + i);
-        __syncwarp();
-        double acc[2][4];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0;
-            const int j = lane + 32 * q;
-            if (j < nbk) {
-                const float ux = (float)(sx[j] * inv), uy = (float)(sy[j] * inv), uz = (float)(sz[j] * inv);
-                float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-                for_regular<P>(ux, uy, uz, [&](int n, int m, float re, float im) {
-                    far_term(srec, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
-                });
-                acc[q][0] = (double)ax * inv;
-                acc[q][1] = (double)ay * inv;
-                acc[q][2] = (double)az * inv;
-                acc[q][3] = (double)ph;
-            }
-        }
+        double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        far_l2p<P>(g, nbk, sx, sy, sz, inv, srec, lane, acc);
         const int total = nbk * nw;
         for (int b0 = 0; b0 < total;) {
-            const int wa = b0 / nbk;
-            const int end = min(total, min(b0 + 32, (wa + FAR_R) * nbk));
-            const int nrec = (end - 1) / nbk - wa + 1;
-            __syncwarp();
-            for (int i = lane; i < nrec * 2 * NEH; i += 32) {
-                const int r = i / (2 * NEH), off = i - r * (2 * NEH);
-                srec[i] = __ldg(hrec + (size_t)tv.w_idx[w0 + wa + r] * 2 * NEH + off);
-            }
-            __syncwarp();
-            const int t = b0 + lane;
-            float4 res = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (t < end) {
-                const int w = t / nbk, j = t - w * nbk;
-                const int c = tv.w_idx[w0 + w];
-                const double2 c01 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c);
-                const double2 c23 = __ldg(reinterpret_cast<const double2*>(tv.center) + 2 * c + 1);
-                const float winv = 1.0f / (2.0f * (float)c23.y);
-                const float ux = (float)(sx[j] + (cx - c01.x)) * winv;
-                const float uy = (float)(sy[j] + (cy - c01.y)) * winv;
-                const float uz = (float)(sz[j] + (cz - c23.x)) * winv;
-                const float4* hr = srec + (w - wa) * 2 * NEH;
-                float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-                for_singular<P + 1>(ux, uy, uz, [&](int n, int m, float re, float im) {
-                    far_term(hr, n * (n + 1) / 2 + m, re, im, ax, ay, az, ph);
-                });
-                const float w2 = winv * winv;
-                res = make_float4(ax * w2, ay * w2, az * w2, POT ? ph * winv : 0.f);
-            }
-            s_res[wid][lane] = res;
-            __syncwarp();
-            const int bm = b0 % nbk;
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int j = lane + 32 * q;
-                if (j < nbk) {
-                    int k = j - bm;
-                    if (k < 0) k += nbk;
-                    for (; b0 + k < end; k += nbk) {
-                        const float4 v = s_res[wid][k];
-                        acc[q][0] += v.x; acc[q][1] += v.y; acc[q][2] += v.z; acc[q][3] += v.w;
-                    }
-                }
-            }
+            const int end = far_round_end(b0, nbk, total);
+            far_m2p_round<P, POT>(tv, hrec, w0, nbk, b0, end, sx, sy, sz, cx, cy, cz, srec, s_res[wid], lane, acc);
             b0 = end;
         }
 #pragma unroll
@@ -748,6 +782,90 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(T
                 double2* o = reinterpret_cast<double2*>(far + 4 * (size_t)(f0 + jb + j));
                 o[0] = make_double2(acc[q][0], acc[q][1]);
                 o[1] = make_double2(acc[q][2], acc[q][3]);
+            }
+        }
+    }
+}
+
+template <int P>
+constexpr size_t far_heavy_smem_bytes() { return FAR_HW * sizeof(float4) * (size_t)far_warp_f4<P>(); }
+
+// list of the leaves with more than FAR_HEAVY M2P tasks (order irrelevant:
+// every leaf's result is computed independently); *count zero before the launch
+__global__ void k_far_heavy_list(TreeView tv, int* __restrict__ list, int* count) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= tv.nleaf) return;
+    if ((int64_t)tv.pcount[tv.leafbox[lf]] * (tv.w_off[lf + 1] - tv.w_off[lf]) > FAR_HEAVY) list[atomicAdd(count, 1)] = lf;
+}
+
+// Leaves with more than FAR_HEAVY M2P tasks: a CTA of FAR_HW warps per leaf,
+// leaves taken from the heavy list through a shared counter (`ctr[1]`, zero
+// before the launch; ctr[0] = list length) so the CTAs balance themselves.  Warp w runs the M2P rounds r = w, w + FAR_HW, ...;
+// warp 0 also the L2P; the warps' per-body partial sums are added in warp order
+// through shared memory (deterministic).
+template <int P, bool POT>
+__global__ void __launch_bounds__(32 * FAR_HW) k_leaf_far32_heavy(TreeView tv, const float4* __restrict__ hrec,
+                                                                 const float4* __restrict__ grec, double* __restrict__ far,
+                                                                 const int* __restrict__ list, int* ctr) {
+    constexpr int NEG = FarRec32<P>::NEG;
+    extern __shared__ float4 s_far_dyn[];
+    __shared__ double s_pos[3][64];
+    __shared__ float4 s_res[FAR_HW][32];
+    __shared__ double s_part[FAR_HW][64][4];
+    __shared__ int s_lf;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(&ctr[1], 1);
+            s_lf = (k < ctr[0]) ? list[k] : -1;
+        }
+        __syncthreads();
+        const int lf = s_lf;
+        if (lf < 0) return;
+        const int b = tv.leafbox[lf];
+        const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+        const int64_t w0 = tv.w_off[lf];
+        const int nw = (int)(tv.w_off[lf + 1] - w0);
+        const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+        const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
+        for (int jb = 0; jb < cnt; jb += 64) {
+            const int nbk = min(64, cnt - jb);
+            __syncthreads();
+            for (int j = threadIdx.x; j < nbk; j += blockDim.x) {
+                const int i = f0 + jb + j;
+                s_pos[0][j] = tv.px[i] - cx;
+                s_pos[1][j] = tv.py[i] - cy;
+                s_pos[2][j] = tv.pz[i] - cz;
+            }
+            __syncthreads();
+            double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+            if (wid == 0) far_l2p<P>(grec + (size_t)lf * 2 * NEG, nbk, s_pos[0], s_pos[1], s_pos[2], inv, srec, lane, acc);
+            const int total = nbk * nw;
+            int r = 0;
+            for (int b0 = 0; b0 < total; ++r) {
+                const int end = far_round_end(b0, nbk, total);
+                if (r % FAR_HW == wid)
+                    far_m2p_round<P, POT>(tv, hrec, w0, nbk, b0, end, s_pos[0], s_pos[1], s_pos[2], cx, cy, cz, srec,
+                                          s_res[wid], lane, acc);
+                b0 = end;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int j = lane + 32 * q;
+                if (j < nbk) {
+                    s_part[wid][j][0] = acc[q][0]; s_part[wid][j][1] = acc[q][1];
+                    s_part[wid][j][2] = acc[q][2]; s_part[wid][j][3] = acc[q][3];
+                }
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < 4 * nbk; t += blockDim.x) {
+                const int j = t >> 2, comp = t & 3;
+                double v = 0.0;
+#pragma unroll
+                for (int w = 0; w < FAR_HW; ++w) v += s_part[w][j][comp];
+                far[4 * (size_t)(f0 + jb + j) + comp] = v;
             }
         }
     }
