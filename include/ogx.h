@@ -95,6 +95,24 @@ int ogx_eval_device(void* handle, int64_t n, const double* d_pos, const double* 
                     double* d_pot);
 int ogx_synchronize(void* handle);
 
+/* FP64 direct summation that allocates no device memory (no counterpart in the reference;
+ * results equal those of ogx_eval on an OGX_SOLVER_DIRECT handle).  For callers that cannot
+ * let a library allocate: cudaMalloc/cudaFree may synchronise the whole device and stall the
+ * caller's other streams, and processes that reserve their device memory up front under a
+ * fixed budget cannot have a library take more.  No handle is needed.
+ * Host buffers: pos n*3 (Vec3 layout), mass n; out acc n*3, pot n or NULL; G and eps as in
+ * KernelParams3D; stream is a cudaStream_t (NULL = the legacy default stream).  Bodies and
+ * results are staged in one fixed array that the library reserves on every GPU it is loaded
+ * on: at most 65536 bodies (4 MiB, held until the process exits); larger n returns
+ * OGX_ERR_INVALID.  The call returns when acc/pot hold the results.
+ * The first call on a device looks up that array's device address (once per device, with
+ * that device current); make that first call before any stream capture.  All calls on a
+ * device share the array: calls that overlap on the GPU (several host threads, or streams
+ * that run at the same time) race, so serialise them.  Nothing in the array has to start at
+ * zero: each call overwrites the inputs it stages and the kernel writes every output. */
+int ogx_direct_eval_noalloc(int64_t n, const double* pos, const double* mass, double G, double eps, double* acc,
+                            double* pot, void* stream);
+
 /* ForceSolver3D::name (src3d/ForceSolver3D.hpp:26). */
 const char* ogx_name(void* handle);
 int ogx_last_stats(void* handle, ogx_stats* out);

@@ -69,6 +69,17 @@ __global__ void __launch_bounds__(DT) k_direct(const double* __restrict__ pos, c
 
 }  // namespace
 
+// FP64 direct sum on caller-provided device buffers and stream (no handle)
+int direct_launch(const double* d_pos, const double* d_mass, int64_t n, double G, double eps2, double* d_acc, double* d_pot,
+                  cudaStream_t st) {
+    if (n == 0) return OGX_OK;
+    const int grid = (int)((n + DT - 1) / DT);
+    if (d_pot) k_direct<double, true><<<grid, DT, 0, st>>>(d_pos, d_mass, n, G, eps2, d_acc, d_pot);
+    else k_direct<double, false><<<grid, DT, 0, st>>>(d_pos, d_mass, n, G, eps2, d_acc, nullptr);
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc, double* d_pot, bool fp32) {
     if (n == 0) return OGX_OK;
     const int grid = (int)((n + DT - 1) / DT);

@@ -201,6 +201,8 @@ int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);
+int direct_launch(const double* d_pos, const double* d_mass, int64_t n, double G, double eps2, double* d_acc, double* d_pot,
+                  cudaStream_t st);
 
 // generic radix sort helpers (ogx_sort.cu)
 int radix_sort_u32(Handle& h, Slot kin, Slot vin, Slot kalt, Slot valt, int64_t n, int bits,

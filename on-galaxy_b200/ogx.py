@@ -31,6 +31,7 @@ EXPORTS = (
     "ogx_params_default", "ogx_create", "ogx_destroy", "ogx_eval", "ogx_eval_device", "ogx_synchronize",
     "ogx_name", "ogx_last_stats", "ogx_strerror", "ogx_last_error_message", "ogx_operator_matrix",
     "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
+    "ogx_direct_eval_noalloc",
 )
 
 
@@ -94,6 +95,7 @@ def load(path: str = LIB_PATH):
     lib.ogx_tree_sizes.argtypes = [vp, C.POINTER(C.c_int64)]
     lib.ogx_tree_boxes.argtypes = [vp, ip, dp, ip]
     lib.ogx_tree_list.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), ip]
+    lib.ogx_direct_eval_noalloc.argtypes = [i64, vp, vp, C.c_double, C.c_double, vp, vp, vp]
     _lib = lib
     return lib
 
@@ -114,6 +116,22 @@ def operator_matrix(kind: int, p: int, index: int) -> np.ndarray:
     _check(load().ogx_operator_matrix(kind, p, index, out.ctypes.data_as(C.POINTER(C.c_double))),
            "ogx_operator_matrix")
     return out.reshape(K, K)
+
+
+NOALLOC_MAX_BODIES = 65536
+
+
+def direct_eval_noalloc(pos, mass, G=1.0, eps=0.0, with_pot=False, stream=None):
+    """FP64 direct sum through ogx_direct_eval_noalloc: no device allocation, at most
+    NOALLOC_MAX_BODIES bodies, host arrays in and out (see include/ogx.h)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    mass = np.ascontiguousarray(mass, dtype=np.float64)
+    n = mass.shape[0]
+    acc = np.zeros((n, 3))
+    pot = np.zeros(n) if with_pot else None
+    _check(load().ogx_direct_eval_noalloc(n, _ptr(pos), _ptr(mass), float(G), float(eps), _ptr(acc), _ptr(pot),
+                                          stream), "ogx_direct_eval_noalloc")
+    return (acc, pot) if with_pot else acc
 
 
 class _Solver:
