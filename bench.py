@@ -43,6 +43,20 @@ THR = 64
 DT = 0.01
 
 
+# DRAM bytes per V-list pair of the tensor-core M2L launch (dram__bytes_read.sum +
+# dram__bytes_write.sum of k_m2l_tc<8> divided by the launch's V-list pairs), from the
+# ncu capture summarised in profiles/k_m2l_tc_merger500k.md; the bytes scale with the
+# pairs a launch processes (sources gathered per pair, results per target).
+M2L_DRAM_BYTES_PER_VPAIR = 22.16
+
+
+def arm_config(n, n_per, world):
+    """The workload both arms are quoted on (the reference arm times a bounded sample of it)."""
+    return {"workload": f"two-galaxy merger, {n} bodies (2x{n_per} disk+bulge), one leapfrog step dt=0.01",
+            "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) before every timed step"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -97,12 +111,12 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "two-galaxy merger (disk+bulge), one force evaluation per system", "p": P_ORDER,
-                   "leaf_capacity": THR, "n_per_system": int(pos.shape[1]), "systems_per_step": threads},
+        "config": arm_config(2 * args.n_per, args.n_per, args.gpus),
         "p50_step_ms": 1e3 * float(np.percentile(times, 50)), "p99_step_ms": 1e3 * float(np.percentile(times, 99)),
         "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": threads, "kind": kind,
-                         "sample": f"{threads} independent {pos.shape[1]}-body mergers per step, AdaptiveFMM3D "
-                                   f"p={P_ORDER} thr={THR}, one per thread"},
+                         "sample": f"{threads} independent {pos.shape[1]}-body mergers per step (same generator, "
+                                   f"2x{n_per} bodies each), one force evaluation of AdaptiveFMM3D p={P_ORDER} "
+                                   f"thr={THR} per system, one system per host thread"},
         "e2e": {"value": value, "unit": "bodies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -298,10 +312,13 @@ def main():
     tc_peak = peaks.get("bf16_tflops", 1590.0)
     K = (P_ORDER + 1) ** 2
     m2l_flops = 2.0 * K * K * st["list_v"] if st["list_v"] else 0.0
-    roofline = {"kernel": "m2l", "bound": "tensor" if prec == ogx.PREC_MIXED else "fp64",
+    traffic = M2L_DRAM_BYTES_PER_VPAIR * st["list_v"] if (M2L_DRAM_BYTES_PER_VPAIR and prec == ogx.PREC_MIXED) else None
+    roofline = {"kernel": "m2l (k_m2l_tc, useful 2K^2 flops per V pair; split precision executes 3x)",
+                "bound": "tensor",
                 "achieved": (m2l_flops / (phases["ms_m2l"] / 1e3) / 1e12) if phases["ms_m2l"] > 0 else None,
-                "peak": tc_peak, "unit": "TFLOP/s", "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback 1.59 PFLOP/s"}
+                "peak": tc_peak, "unit": "TFLOP/s", "traffic": traffic,
+                "peak_source": ("MEASURED_PEAKS.json bf16_tflops (of measured)" if peaks else
+                                "fallback 1.59 PFLOP/s (of fallback)")}
     if roofline["achieved"] is not None:
         roofline["frac"] = roofline["achieved"] / roofline["peak"]
 
@@ -310,9 +327,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "mixed(f32 P2P, 3xTF32 M2L, f64 translations)" if prec == ogx.PREC_MIXED else "f64",
         "data": "synthetic",
-        "config": {"workload": f"two-galaxy merger, {n} bodies (2x{args.n_per} disk+bulge), one leapfrog step dt=0.01",
-                   "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MiB write) before every timed step"},
+        "config": arm_config(n, args.n_per, world),
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
         "e2e": {"value": world * n / (e2e_mean / 1e3), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
                 "d2h_bytes_per_step": int(24 * n), "ms_per_step": e2e_mean},
