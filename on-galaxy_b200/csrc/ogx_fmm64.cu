@@ -473,7 +473,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         }
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));
-    k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
+    if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }
+    else { k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
     OGX_TRY(launch_l2l<P>(h, L, Lown));
     OGX_CUDA(cudaEventRecord(h.ev[6], st));

@@ -871,5 +871,77 @@ __global__ void __launch_bounds__(32 * FAR_HW) k_leaf_far32_heavy(TreeView tv, c
     }
 }
 
+// ---- P2L over X lists in FP32 (p <= 9) ------------------------------------------------
+// L_b += sum over the X-list leaves c of b, bodies j of c: q_j S_n^m(x_j - c_b)
+// (AdaptiveFMM3D::p2lAccum, src3d/AdaptiveFMM3D.hpp:117-128, scaled by side^n).
+// Warp per box (one warp per block).  The bodies of all X-list leaves form one
+// flat sequence; lane l takes positions l, l + 32, ... walking the entries on its
+// own, so every lane evaluates a body each round however the leaves are sized.
+// Each lane sums its K coefficients in registers (FP32); the 32 lane sums are
+// added once per box through shared memory in FP64.
+template <int P>
+struct P2L32 {
+    static constexpr int K = (P + 1) * (P + 1);
+    static constexpr bool OK = K <= 100;   // register budget of the per-lane sums
+};
+
+template <int P>
+__global__ void __launch_bounds__(32, 16) k_p2l32(TreeView tv, double* __restrict__ lown) {
+    constexpr int K = (P + 1) * (P + 1);
+    constexpr int LD = K | 1;
+    constexpr int NPL = (K + 31) / 32;
+    __shared__ float s_red[32 * LD];
+    const int lane = threadIdx.x;
+    const int b = blockIdx.x;
+    const int64_t e0 = tv.x_off[b], e1 = tv.x_off[b + 1];
+    if (e0 == e1) return;
+    const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
+    const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
+    float acc[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) acc[d] = 0.f;
+    int64_t e = e0;
+    int c = tv.x_idx[e];
+    int f0 = tv.pfirst[c], cnt = tv.pcount[c];
+    int j = lane;
+    for (;;) {
+        while (e < e1 && j >= cnt) {
+            j -= cnt;
+            if (++e < e1) {
+                c = tv.x_idx[e];
+                f0 = tv.pfirst[c];
+                cnt = tv.pcount[c];
+            }
+        }
+        const bool act = e < e1;
+        if (!__any_sync(0xffffffffu, act)) break;
+        if (act) {
+            const int i = f0 + j;
+            const float q = (float)tv.pm[i];
+            const float ux = (float)((tv.px[i] - cx) * inv), uy = (float)((tv.py[i] - cy) * inv),
+                        uz = (float)((tv.pz[i] - cz) * inv);
+            for_singular<P>(ux, uy, uz, [&](int n, int m, float re, float im) {
+                const int dr = dof_re(n, m);
+                acc[dr] = fmaf(q, re, acc[dr]);
+                if (m > 0) acc[dr + 1] = fmaf(-q, im, acc[dr + 1]);
+            });
+        }
+        j += 32;
+    }
+#pragma unroll
+    for (int d = 0; d < K; ++d) s_red[lane * LD + d] = acc[d];
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NPL; ++q) {
+        const int d = lane + 32 * q;
+        if (d < K) {
+            double sum = 0.0;
+#pragma unroll 8
+            for (int r = 0; r < 32; ++r) sum += (double)s_red[r * LD + d];
+            lown[(size_t)b * K + d] += sum * inv;
+        }
+    }
+}
+
 }  // namespace mixed
 }  // namespace ogx
