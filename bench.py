@@ -57,6 +57,22 @@ def arm_config(n, n_per, world):
             "l2": "flushed (256 MiB write) before every timed step"}
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank float over all ranks (the value itself without a process group).
+    Works with NCCL (device "cuda") and gloo (device "cpu")."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(n_per_rank, world, ms_per_step):
+    """Whole-job bodies/s of `world` independent replicas timed at the slowest rank's step."""
+    return world * n_per_rank / (ms_per_step / 1e3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,13 +267,9 @@ def main():
         barrier()
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     my_ms = float(step_ms.sum())
-    tot_ms = my_ms
-    if dist is not None:
-        t = torch.tensor([my_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(my_ms, dist, "cuda")
     ms_per_step = tot_ms / args.steps
-    value = world * n / (ms_per_step / 1e3)
+    value = replica_value(n, world, ms_per_step)
     st = phase[-1]
 
     # ---- e2e through the C ABI with pinned host buffers
@@ -275,11 +287,7 @@ def main():
         b.record(stream)
         b.synchronize()
         e2e_ms.append(a.elapsed_time(b))
-    e2e_mean = float(np.mean(e2e_ms))
-    if dist is not None:
-        t = torch.tensor([e2e_mean], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_mean = float(t.item())
+    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)), dist, "cuda")
 
     # ---- accuracy on the evaluated configuration (untimed)
     acc_info = {}
@@ -329,7 +337,7 @@ def main():
         "data": "synthetic",
         "config": arm_config(n, args.n_per, world),
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
-        "e2e": {"value": world * n / (e2e_mean / 1e3), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
+        "e2e": {"value": replica_value(n, world, e2e_mean), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
                 "d2h_bytes_per_step": int(24 * n), "ms_per_step": e2e_mean},
         "phases_ms": phases, "tree": {k: st[k] for k in ("num_boxes", "num_leaves", "max_level", "max_leaf_occupancy",
                                                           "list_u", "list_v", "list_w", "p2p_pairs", "m2p_evals")},
