@@ -146,6 +146,47 @@ int ogx_tree_sizes(void* handle, int64_t* sizes);
 int ogx_tree_boxes(void* handle, int32_t* boxes, double* centers, int32_t* perm);
 int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx);
 
+/* ---- running a simulation on the device ---------------------------------------------- */
+
+/* Two-galaxy merger initial conditions.  Replaces makeDisk / setCircularVelocities /
+ * placeGalaxy / concat (src3d/gpu/GalaxyIC.hpp:43-125) and the merger set-up of galaxy_sim
+ * (src3d/gpu/galaxy_sim.cu:113-137).  Each galaxy: (1 - bulge_frac) of the bodies in an
+ * exponential sech^2 disk (Rd, z0, mass Md; cut at 10 Rd and 10 z0), bulge_frac in a
+ * Hernquist bulge (ab, Mb; cut at 50 ab).  Velocities: v_c^2 = -a_R R from the FP64 field of
+ * the galaxy alone, plus Gaussian dispersion disp_frac * v_c.  Galaxy 0 sits at x = -sep with
+ * bulk velocity +vrel/2, galaxy 1 at x = +sep with -vrel/2, tilted by tilt_deg about x. */
+typedef struct {
+    int64_t n_per;       /* bodies per galaxy */
+    uint64_t seed;
+    double sep, vrel, tilt_deg, disp_frac;
+    double Rd, z0, Md, ab, Mb, bulge_frac;
+} ogx_merger_params;
+
+/* Defaults of the 1M benchmark merger: n_per 500000, seed 1, sep 5, vrel 0.5, tilt 30,
+ * dispersion 0.1, Rd 1, z0 0.1, Md 1, ab 0.2, Mb 0.25, bulge 20%. */
+int ogx_merger_params_default(ogx_merger_params* mp);
+
+/* Generate the merger on the device straight into the handle's resident state (as
+ * ogx_upload, including VelocityVerlet3D::initialize), bodies in galaxy order; the species
+ * tag of a body is its galaxy (0 or 1), as galaxy_sim tags them.  species_out: NULL or n int8. */
+int ogx_ic_merger(void* handle, const ogx_merger_params* mp, int8_t* species_out);
+
+/* Species tags of the resident bodies (n int8, host), used by ogx_diagnostics. */
+int ogx_set_species(void* handle, const int8_t* species);
+
+/* Diagnostics of the resident state.  Replaces computeDiagnostics (src3d/Diagnostics3D.hpp:20-38)
+ * and comSep (src3d/gpu/galaxy_sim.cu:209-216).  FP64 sums in a fixed order; the potential
+ * energy is 1/2 sum m_i pot_i from a force evaluation with potentials at the current
+ * positions (the reference sums -G m_i m_j / sqrt(r^2 + eps^2) over pairs; with this
+ * library's solvers the far field is unsoftened, as in AdaptiveFMM3D).
+ * out[16]: kinetic, potential, total, momentum xyz, angular momentum xyz, centre of mass of
+ * species 0 xyz, of the other species xyz, their separation. */
+int ogx_diagnostics(void* handle, double* out);
+
+/* Resident positions as float32, n*3 in original body order: one frame of the reference's
+ * frames.bin (src3d/gpu/galaxy_sim.cu:186-193). */
+int ogx_download_frame(void* handle, float* pos_f32);
+
 #ifdef __cplusplus
 }
 #endif

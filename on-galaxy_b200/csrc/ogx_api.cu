@@ -573,3 +573,11 @@ int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx) {
 namespace ogx {
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 }
+
+namespace ogx {
+// entry points for the other C-ABI files (run support in ogx_run.cu)
+int eval_device_shared(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+    return eval_device(h, n, d_pos, d_mass, d_acc, d_pot);
+}
+void finish_stats_shared(Handle& h) { finish_stats(h); }
+}  // namespace ogx

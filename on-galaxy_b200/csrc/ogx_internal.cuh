@@ -76,6 +76,7 @@ enum Slot {
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_FAR_HEAVY,
+    S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
     S_NUM_SLOTS
 };
 
@@ -165,6 +166,7 @@ struct Handle {
     double* d_l2l = nullptr;  // 8 x K x K
     // device-resident integrator state
     bool resident = false;
+    bool species_set = false;       // species tags uploaded (or made by ogx_ic_merger)
     cudaEvent_t ev[12] = {};
     TreeView tv{};
     bool tree_valid = false;
@@ -201,6 +203,8 @@ int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);
+int eval_device_shared(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot);
+void finish_stats_shared(Handle& h);
 int direct_launch(const double* d_pos, const double* d_mass, int64_t n, double G, double eps2, double* d_acc, double* d_pot,
                   cudaStream_t st);
 

@@ -31,7 +31,8 @@ EXPORTS = (
     "ogx_params_default", "ogx_create", "ogx_destroy", "ogx_eval", "ogx_eval_device", "ogx_synchronize",
     "ogx_name", "ogx_last_stats", "ogx_strerror", "ogx_last_error_message", "ogx_operator_matrix",
     "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
-    "ogx_direct_eval_noalloc",
+    "ogx_direct_eval_noalloc", "ogx_merger_params_default", "ogx_ic_merger", "ogx_set_species",
+    "ogx_diagnostics", "ogx_download_frame",
 )
 
 
@@ -52,6 +53,16 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class MergerParams(C.Structure):
+    _fields_ = [("n_per", C.c_int64), ("seed", C.c_uint64), ("sep", C.c_double), ("vrel", C.c_double),
+                ("tilt_deg", C.c_double), ("disp_frac", C.c_double), ("Rd", C.c_double), ("z0", C.c_double),
+                ("Md", C.c_double), ("ab", C.c_double), ("Mb", C.c_double), ("bulge_frac", C.c_double)]
+
+
+DIAG_FIELDS = ("kinetic", "potential", "total", "px", "py", "pz", "lx", "ly", "lz",
+               "com0_x", "com0_y", "com0_z", "com1_x", "com1_y", "com1_z", "sep")
 
 
 class OgxError(RuntimeError):
@@ -96,6 +107,11 @@ def load(path: str = LIB_PATH):
     lib.ogx_tree_boxes.argtypes = [vp, ip, dp, ip]
     lib.ogx_tree_list.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), ip]
     lib.ogx_direct_eval_noalloc.argtypes = [i64, vp, vp, C.c_double, C.c_double, vp, vp, vp]
+    lib.ogx_merger_params_default.argtypes = [C.POINTER(MergerParams)]
+    lib.ogx_ic_merger.argtypes = [vp, C.POINTER(MergerParams), vp]
+    lib.ogx_set_species.argtypes = [vp, vp]
+    lib.ogx_diagnostics.argtypes = [vp, dp]
+    lib.ogx_download_frame.argtypes = [vp, vp]
     _lib = lib
     return lib
 
@@ -218,6 +234,33 @@ class _Solver:
         pos, vel, acc = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
         _check(self._lib.ogx_download(self._h, _ptr(pos), _ptr(vel), _ptr(acc)), "ogx_download")
         return pos, vel, acc
+
+    # running a simulation on the device
+    def ic_merger(self, n_per, seed=1, **kw):
+        """Generate the two-galaxy merger on the device into the resident state; returns species (galaxy tags)."""
+        mp = MergerParams()
+        _check(self._lib.ogx_merger_params_default(C.byref(mp)), "ogx_merger_params_default")
+        mp.n_per, mp.seed = int(n_per), int(seed)
+        for k, v in kw.items():
+            setattr(mp, k, v)
+        species = np.zeros(2 * int(n_per), np.int8)
+        _check(self._lib.ogx_ic_merger(self._h, C.byref(mp), _ptr(species)), "ogx_ic_merger")
+        self._n = species.shape[0]
+        return species
+
+    def set_species(self, species):
+        species = np.ascontiguousarray(species, np.int8)
+        _check(self._lib.ogx_set_species(self._h, _ptr(species)), "ogx_set_species")
+
+    def diagnostics(self) -> dict:
+        out = np.zeros(len(DIAG_FIELDS))
+        _check(self._lib.ogx_diagnostics(self._h, out.ctypes.data_as(C.POINTER(C.c_double))), "ogx_diagnostics")
+        return dict(zip(DIAG_FIELDS, out.tolist()))
+
+    def download_frame(self):
+        frame = np.zeros((self._n, 3), np.float32)
+        _check(self._lib.ogx_download_frame(self._h, _ptr(frame)), "ogx_download_frame")
+        return frame
 
     def tree(self):
         """Tree of the last evaluation in the same layout as the oracle export."""
