@@ -1,10 +1,14 @@
 // ogx_lists.cu -- Carrier-Greengard-Rokhlin interaction lists on the GPU.
 //
 // Replaces AdaptiveOctree::buildLists (src3d/AdaptiveOctree.hpp:137-189):
-//  - colleagues: same-level adjacent boxes, taken from the children of the
-//    parent's colleagues (:143-151).  Parent-centric: a warp per parent, lanes
-//    over its 27 colleague slots, each lane places the children of its
-//    colleague into the children's slots (slot = integer offset in [-1,1]^3);
+//  - colleagues: same-level adjacent boxes, the children of the parent's
+//    colleagues that pass `adjacent` (:143-151).  Box centres are exact binary
+//    fractions of the root box, so for same-level boxes that test holds exactly
+//    for integer offsets in [-1,1]^3: every (box, slot) finds its colleague in
+//    one launch by a binary search of the level's boxes (Morton order) for the
+//    offset coordinates.  A second launch replays the reference's recursion over
+//    the children of each parent's colleagues with the FP64 predicate and counts
+//    every disagreement with the search (expected 0);
 //  - V is implicit: children of the parent's colleagues at integer offset
 //    max|o| >= 2 (:154-161); every candidate is also classified with the
 //    reference's FP64 predicate and disagreements are counted (expected 0);
@@ -15,6 +19,8 @@
 //    members and the W boxes).  A count pass sizes the CSR, a fill pass writes
 //    each lane's items at its warp-scan offset, so the order is deterministic;
 //  - X = transpose of W through a stable sort by W member (:171-173).
+#include <algorithm>
+
 #include "ogx_tree_common.cuh"
 
 namespace ogx {
@@ -23,14 +29,55 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int UW_STACK = 192;
 
-__global__ void k_root_col(int* col) {
-    const int d = threadIdx.x;
-    if (d < 27) col[d] = (d == 13) ? 0 : -1;
+struct LevelOffsets {
+    int off[kMaxDepth + 2];   // first box of each level, off[l + 1] = end of level l
+};
+
+// p's highest set bit is below q's
+__device__ __forceinline__ bool msb_less(unsigned p, unsigned q) { return p < q && p < (p ^ q); }
+
+// Morton order of two boxes of one level from their integer coordinates: the
+// dimension whose coordinates first differ at the highest bit decides; at equal
+// bits z ranks above y above x (octant digit = x | y << 1 | z << 2)
+__device__ __forceinline__ bool morton_less(int ax, int ay, int az, int bx, int by, int bz) {
+    const unsigned x = (unsigned)(ax ^ bx), y = (unsigned)(ay ^ by), z = (unsigned)(az ^ bz);
+    int d = 2;
+    unsigned m = z;
+    if (msb_less(m, y)) { d = 1; m = y; }
+    if (msb_less(m, x)) d = 0;
+    return d == 0 ? ax < bx : (d == 1 ? ay < by : az < bz);
 }
 
-__global__ void __launch_bounds__(128) k_colleagues_par(int first, int count, const int* __restrict__ leafid,
-                                                        const int* __restrict__ child, const double* __restrict__ ctr,
-                                                        const RootInfo* root, int* col, DevCounts* counts) {
+// colleague slot d of box b: the box of b's level at integer offset (d % 3 - 1, ...)
+__global__ void k_colleagues_bs(int nb, LevelOffsets lv, const int* __restrict__ level, const int* __restrict__ coord,
+                                int* __restrict__ col) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 27 * (int64_t)nb) return;
+    const int b = (int)(t / 27), d = (int)(t - 27 * (int64_t)b);
+    if (d == 13) { col[t] = b; return; }
+    const int l = level[b];
+    const int side = 1 << l;
+    const int nx = coord[3 * b] + d % 3 - 1, ny = coord[3 * b + 1] + (d / 3) % 3 - 1, nz = coord[3 * b + 2] + d / 9 - 1;
+    int found = -1;
+    if (l > 0 && nx >= 0 && ny >= 0 && nz >= 0 && nx < side && ny < side && nz < side) {
+        int lo = lv.off[l], hi = lv.off[l + 1] - 1;
+        while (lo <= hi) {
+            const int mid = (lo + hi) >> 1;
+            const int mx = coord[3 * mid], my = coord[3 * mid + 1], mz = coord[3 * mid + 2];
+            if (mx == nx && my == ny && mz == nz) { found = mid; break; }
+            if (morton_less(mx, my, mz, nx, ny, nz)) lo = mid + 1;
+            else hi = mid - 1;
+        }
+    }
+    col[t] = found;
+}
+
+// the reference's recursion (children of the parent's colleagues, FP64 `adjacent`)
+// checked against the searched colleagues; also counts the V-list pairs
+__global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, const int* __restrict__ leafid,
+                                                          const int* __restrict__ child, const double* __restrict__ ctr,
+                                                          const RootInfo* root, const int* __restrict__ col,
+                                                          DevCounts* counts) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * 4 + wid;
     if (k >= count) return;
@@ -57,7 +104,7 @@ __global__ void __launch_bounds__(128) k_colleagues_par(int first, int count, co
                               oz = 2 * Dz + ((s >> 2) & 1) - ((t >> 2) & 1);
                     const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
                     if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
-                    if (adj_i) col[27 * b + colleague_slot(ox, oy, oz)] = c;
+                    if (adj_i) { if (col[27 * b + colleague_slot(ox, oy, oz)] != c) ++mism; }
                     else ++nv;
                 }
             }
@@ -257,12 +304,10 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
     int* col;
     OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
-    OGX_CUDA(cudaMemsetAsync(col, 0xFF, 27 * sizeof(int) * (size_t)nb, st));
-    k_root_col<<<1, 32, 0, st>>>(col); ++h.launches;
-    for (int l = 1; l <= h.max_level; ++l) {
-        const int first = h.level_off[l - 1], count = h.level_off[l] - first;
-        k_colleagues_par<<<grid_for(count, 4), 128, 0, st>>>(first, count, tv.leafid, tv.child, tv.center, tv.root, col, dc); ++h.launches;
-    }
+    LevelOffsets lv{};
+    for (int l = 0; l <= h.max_level + 1 && l < kMaxDepth + 2; ++l) lv.off[l] = h.level_off[std::min<int>(l, (int)h.level_off.size() - 1)];
+    k_colleagues_bs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, st>>>(nb, lv, tv.level, tv.coord, col); ++h.launches;
+    k_colleagues_check<<<grid_for(nb, 4), 128, 0, st>>>(0, nb, tv.leafid, tv.child, tv.center, tv.root, col, dc); ++h.launches;
     tv.col = col;
 
     int *ucnt, *wcnt, *lane_uw;

@@ -1,0 +1,57 @@
+"""Config 2 at full size: a 262,144-body disk+bulge galaxy (80% exponential sech^2 disk,
+20% Hernquist bulge), p in {4, 8, 12}, leaf capacity 32-128, FP64 and mixed forms.
+
+The CPU oracle cannot run this size in seconds, so the checks are size-independent:
+  * the FP64 form converges with p against the GPU FP64 direct sum (itself equal to
+    DirectSolver3D to 1e-12, see test_gpu_fp64.py), with RMS errors at the level the
+    reference's operators reach (1.3e-3 / 1.3e-5 / 5e-7 at p = 4 / 8 / 12 on
+    a Plummer sphere);
+  * the mixed form stays within the mixed tolerance of the FP64 form at every p and
+    leaf capacity (it must not add error on top of the truncation error);
+  * trees are consistent: every body in exactly one leaf, no leaf above capacity unless
+    at the depth cap.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+N = 262144
+MIXED_TOL = 5e-6
+
+
+def _rms(ref, got):
+    a = np.linalg.norm(ref, axis=1)
+    e = np.linalg.norm(got - ref, axis=1)
+    return float(np.sqrt((e * e).sum() / (a * a).sum()))
+
+
+@pytest.fixture(scope="module")
+def galaxy(ogx):
+    import ogx_ic
+    pos, mass, _ = ogx_ic.disk_bulge(N, seed=11)
+    with ogx.DirectSolver3D() as d:
+        ref = d.compute_accelerations(pos, mass)
+    return pos, mass, ref
+
+
+@pytest.mark.parametrize("p,bound", [(4, 5e-3), (8, 1e-4), (12, 5e-6)])
+def test_fp64_form_converges_with_p(ogx, galaxy, p, bound):
+    pos, mass, ref = galaxy
+    with ogx.AdaptiveFMM3D(p=p, threshold=64, precision=ogx.PREC_FP64) as s:
+        acc = s.compute_accelerations(pos, mass)
+        st = s.stats()
+    assert _rms(ref, acc) < bound
+    assert st["max_leaf_occupancy"] <= 64 and st["adjacency_mismatch"] == 0
+
+
+@pytest.mark.parametrize("p,thr", [(4, 64), (8, 32), (8, 64), (8, 128), (12, 64)])
+def test_mixed_form_tracks_fp64_form(ogx, galaxy, p, thr):
+    pos, mass, _ = galaxy
+    with ogx.AdaptiveFMM3D(p=p, threshold=thr, precision=ogx.PREC_FP64) as s:
+        a64 = s.compute_accelerations(pos, mass)
+    with ogx.AdaptiveFMM3D(p=p, threshold=thr, precision=ogx.PREC_MIXED) as s:
+        amx = s.compute_accelerations(pos, mass)
+        st = s.stats()
+    assert _rms(a64, amx) < MIXED_TOL
+    assert st["max_leaf_occupancy"] <= thr
