@@ -143,7 +143,23 @@ __global__ void k_kick(double* vel, const double* acc_old, const double* acc_new
 
 static int device_error(Handle& h);
 
+static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot);
+
+// Every evaluation runs on the handle's internal high-priority stream: ordered
+// after the caller's stream's earlier work and before its later work.
 static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
+    const cudaStream_t user = h.stream;
+    OGX_CUDA(cudaEventRecord(h.ev_in, user));
+    OGX_CUDA(cudaStreamWaitEvent(h.main, h.ev_in, 0));
+    h.stream = h.main;
+    const int rc = eval_device_on(h, n, d_pos, d_mass, d_acc, d_pot);
+    h.stream = user;
+    OGX_CUDA(cudaEventRecord(h.ev_out, h.main));
+    OGX_CUDA(cudaStreamWaitEvent(user, h.ev_out, 0));
+    return rc;
+}
+
+static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {
     h.n = n;
     h.tree_valid = false;
     std::memset(&h.stats, 0, sizeof(h.stats));
@@ -162,6 +178,10 @@ static int eval_device(Handle& h, int64_t n, const double* d_pos, const double* 
     OGX_TRY(ensure_operator_tables(h));
     OGX_TRY(tree_build(h, d_pos, d_mass, n));
     OGX_CUDA(cudaEventRecord(h.ev[1], st));
+    // mixed form: the upward pass needs only the tree, so it runs on its own stream
+    // while the lists are built
+    h.upward_split = (h.prm.precision == OGX_PREC_MIXED);
+    if (h.upward_split) OGX_TRY(fmm_mixed_upward(h));
     OGX_TRY(lists_build(h));
     OGX_CUDA(cudaEventRecord(h.ev[9], st));
     h.tree_valid = true;
@@ -203,7 +223,7 @@ static void finish_stats(Handle& h) {
     if (h.prm.solver == OGX_SOLVER_DIRECT) return;
     s.ms_tree = ev_ms(h.ev[0], h.ev[1]);
     s.ms_lists = ev_ms(h.ev[1], h.ev[9]);
-    s.ms_upward = ev_ms(h.ev[2], h.ev[3]);
+    s.ms_upward = ev_ms(h.ev[2], h.upward_split ? h.ev_up_end : h.ev[3]);
     s.ms_m2l = ev_ms(h.ev[3], h.ev[4]);
     s.ms_p2l = ev_ms(h.ev[4], h.ev[5]);
     s.ms_downward = ev_ms(h.ev[5], h.ev[6]);
@@ -282,6 +302,14 @@ int ogx_create(const ogx_params* prm, void** handle) {
     *h->h_err = 0;
     std::memset(h->h_counts, 0, sizeof(DevCounts));
     for (auto& e : h->ev) OGX_CUDA(cudaEventCreate(&e));
+    int prio_low = 0, prio_high = 0;
+    OGX_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    OGX_CUDA(cudaStreamCreateWithPriority(&h->main, cudaStreamNonBlocking, prio_high));
+    OGX_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_low));
+    OGX_CUDA(cudaStreamCreateWithPriority(&h->up, cudaStreamNonBlocking, prio_high));
+    for (cudaEvent_t* e : {&h->ev_fork, &h->ev_join, &h->ev_in, &h->ev_out, &h->ev_tree, &h->ev_up})
+        OGX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    OGX_CUDA(cudaEventCreate(&h->ev_up_end));
     *handle = h.release();
     return OGX_OK;
 }
@@ -297,6 +325,13 @@ int ogx_destroy(void* handle) {
         if (h->h_err) cudaFreeHost(h->h_err);
         if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto& e : h->ev)
+            if (e) cudaEventDestroy(e);
+        for (cudaStream_t sx : {h->main, h->side, h->up})
+            if (sx) {
+                cudaStreamSynchronize(sx);
+                cudaStreamDestroy(sx);
+            }
+        for (cudaEvent_t e : {h->ev_fork, h->ev_join, h->ev_in, h->ev_out, h->ev_tree, h->ev_up, h->ev_up_end})
             if (e) cudaEventDestroy(e);
         if (h->own_stream) cudaStreamDestroy(h->stream);
     }

@@ -91,7 +91,8 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
 //   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
 constexpr int TR_PB = 2;   // parents per CTA
 template <int P, int MODE>
-__global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* __restrict__ parents, int count,
+__global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* __restrict__ nonleaf,
+                                                       const int* __restrict__ nl_off, int level,
                                                        const double* __restrict__ opsT, double* mpole, double* local,
                                                        const double* __restrict__ lown) {
     constexpr int K = (P + 1) * (P + 1);
@@ -99,7 +100,12 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
     __shared__ double s_in[MODE == 0 ? 8 : 1][TR_PB][K];
     __shared__ double s_part[MODE == 0 ? 8 : 1][TR_PB][MODE == 0 ? K : 1];
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    // this level's non-leaf parents (count known on the device only; the grid is
+    // sized for all boxes of the level)
+    const int first = nl_off[level], count = nl_off[level + 1] - first;
+    const int* parents = nonleaf + first;
     const int p0 = blockIdx.x * TR_PB;
+    if (p0 >= count) return;
     int bx[TR_PB], ch[TR_PB];
     bool any = false;
 #pragma unroll
@@ -178,8 +184,8 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
 template <int P>
 int launch_m2m(Handle& h, double* M) {
     for (int l = h.max_level - 1; l >= 0; --l) {
-        const int first = h.nonleaf_off[l], count = h.nonleaf_off[l + 1] - first;
-        if (count > 0) { k_translate_oct<P, 0><<<(count + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf + first, count, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+        const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
+        if (nbl > 0) { k_translate_oct<P, 0><<<(nbl + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -191,8 +197,8 @@ int launch_l2l(Handle& h, double* L, const double* Lown) {
     OGX_CUDA(cudaMemcpyAsync(L + (size_t)h.level_off[0] * K, Lown + (size_t)h.level_off[0] * K, sizeof(double) * K,
                              cudaMemcpyDeviceToDevice, h.stream));
     for (int l = 0; l < h.max_level; ++l) {
-        const int first = h.nonleaf_off[l], count = h.nonleaf_off[l + 1] - first;
-        if (count > 0) { k_translate_oct<P, 1><<<(count + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf + first, count, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+        const int nbl = h.level_off[l + 1] - h.level_off[l];
+        if (nbl > 0) { k_translate_oct<P, 1><<<(nbl + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -424,6 +430,41 @@ int ensure_mixed_tables(Handle& h) {
     return OGX_OK;
 }
 
+// Mixed-form upward pass (P2M, M2M, TF32 split of the multipoles) on h.up, forked
+// from the main stream right after the tree build; the main stream joins it
+// (h.ev_up) before the M2L.
+template <int P>
+int run_mixed_upward(Handle& h) {
+    using C = mixed::TcCfg<P>;
+    constexpr int K = (P + 1) * (P + 1);
+    TreeView& tv = h.tv;
+    OGX_TRY(harm_tables_ready(h.device));
+    if constexpr (C::SUPPORTED) OGX_TRY(ensure_mixed_tables<P>(h));
+    double* M;
+    float *mhi, *mlo;
+    OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
+    OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
+    OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
+    const size_t p2x_smem = p2x_smem_bytes<P, float>();
+    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(cudaEventRecord(h.ev_tree, h.stream));
+    const cudaStream_t main_st = h.stream, su = h.up;
+    OGX_CUDA(cudaStreamWaitEvent(su, h.ev_tree, 0));
+    h.stream = su;   // launch_m2m issues on h.stream
+    OGX_CUDA(cudaEventRecord(h.ev[2], su));
+    k_p2x<P, 0, float><<<(tv.nleaf + 3) / 4, 128, p2x_smem, su>>>(tv, tv.nleaf, M); ++h.launches;
+    const int rc = launch_m2m<P>(h, M);
+    h.stream = main_st;
+    OGX_TRY(rc);
+    if constexpr (C::SUPPORTED) {
+        const int64_t tot = (int64_t)tv.nb * C::KPAD;
+        mixed::k_split_mpole<P><<<(int)((tot + 255) / 256), 256, 0, su>>>(M, tv.nb, mhi, mlo); ++h.launches;
+    }
+    OGX_CUDA(cudaEventRecord(h.ev_up_end, su));
+    OGX_CUDA(cudaEventRecord(h.ev_up, su));
+    return OGX_OK;
+}
+
 template <int P>
 int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     using C = mixed::TcCfg<P>;
@@ -431,8 +472,6 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     constexpr int LD = K | 1;
     const cudaStream_t st = h.stream;
     TreeView& tv = h.tv;
-    OGX_TRY(harm_tables_ready(h.device));
-    if constexpr (C::SUPPORTED) OGX_TRY(ensure_mixed_tables<P>(h));
     double *M, *L, *Lown, *far;
     float *mhi, *mlo;
     OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
@@ -441,17 +480,12 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
     OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
-    OGX_CUDA(cudaEventRecord(h.ev[2], st));
-    // upward (FP64)
+    double* nearb;
+    OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
-    k_p2x<P, 0, float><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
-    OGX_TRY(launch_m2m<P>(h, M));
-    {
-        const int64_t tot = (int64_t)tv.nb * C::KPAD;
-        if constexpr (C::SUPPORTED) { mixed::k_split_mpole<P><<<(int)((tot + 255) / 256), 256, 0, st>>>(M, tv.nb, mhi, mlo); ++h.launches; }
-    }
+    // join the upward pass
+    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
     // M2L on the tensor cores
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
@@ -473,6 +507,16 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         }
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));
+    // near field on the low-priority side stream, after the M2L (which needs whole
+    // SMs): it fills what P2L, L2L and the far field leave idle
+    {
+        const float eps2 = (float)(h.prm.eps * h.prm.eps);
+        OGX_CUDA(cudaEventRecord(h.ev_fork, st));
+        OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
+        if (d_pot) { mixed::k_leaf_near32<true><<<tv.nleaf, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
+        else { mixed::k_leaf_near32<false><<<tv.nleaf, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
+        OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
+    }
     if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }
     else { k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
@@ -480,10 +524,11 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaEventRecord(h.ev[6], st));
     const bool pot = d_pot != nullptr;
     OGX_TRY(launch_far32<P>(h, M, L, far, pot));
+    // join the near field, then acc = G (far + near) in the caller's order
+    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_join, 0));
     const double G = h.prm.G;
-    const float eps2 = (float)(h.prm.eps * h.prm.eps);
-    if (pot) { mixed::k_leaf_near32<true><<<tv.nleaf, 32, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
-    else { mixed::k_leaf_near32<false><<<tv.nleaf, 32, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
+    if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, d_pot); ++h.launches; }
+    else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, nullptr); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[7], st));
     OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaGetLastError());
@@ -491,6 +536,24 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
 }
 
 }  // namespace
+
+int fmm_mixed_upward(Handle& h) {
+    switch (h.prm.p) {
+        case 1: return run_mixed_upward<1>(h);
+        case 2: return run_mixed_upward<2>(h);
+        case 3: return run_mixed_upward<3>(h);
+        case 4: return run_mixed_upward<4>(h);
+        case 5: return run_mixed_upward<5>(h);
+        case 6: return run_mixed_upward<6>(h);
+        case 7: return run_mixed_upward<7>(h);
+        case 8: return run_mixed_upward<8>(h);
+        case 9: return run_mixed_upward<9>(h);
+        case 10: return run_mixed_upward<10>(h);
+        case 11: return run_mixed_upward<11>(h);
+        case 12: return run_mixed_upward<12>(h);
+        default: return OGX_ERR_INVALID;
+    }
+}
 
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot) {
     switch (h.prm.p) {

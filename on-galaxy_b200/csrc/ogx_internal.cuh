@@ -75,8 +75,8 @@ enum Slot {
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
-    S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_FAR_HEAVY,
-    S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
+    S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,
+    S_NEAR32, S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
     S_NUM_SLOTS
 };
 
@@ -168,6 +168,14 @@ struct Handle {
     bool resident = false;
     bool species_set = false;       // species tags uploaded (or made by ogx_ic_merger)
     cudaEvent_t ev[12] = {};
+    // side stream for work that overlaps the main chain (joined back before returning)
+    // internal streams: the evaluation runs on `main` (highest priority), forked
+    // from and joined back to the caller's stream; overlapping work goes to `side`
+    // (lowest priority) so it only fills SMs the main chain leaves idle
+    cudaStream_t main = nullptr, side = nullptr, up = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_in = nullptr, ev_out = nullptr, ev_tree = nullptr, ev_up = nullptr;
+    cudaEvent_t ev_up_end = nullptr;   // timing: end of an upward pass that ran on `up`
+    bool upward_split = false;         // the last evaluation ran its upward pass on `up`
     TreeView tv{};
     bool tree_valid = false;
     // mixed-precision tables
@@ -185,7 +193,7 @@ struct Handle {
     const uint32_t* tgt_tile_box = nullptr;
     // non-leaf boxes, level-major (M2M / L2L parents); nonleaf_off[l] = first of level l
     const int* d_nonleaf = nullptr;
-    std::vector<int32_t> nonleaf_off;
+    const int* d_nonleaf_off = nullptr;   // device, kMaxDepth + 2 entries
 };
 
 // ---- host-side operator tables (ogx_tables.cpp) -----------------------------
@@ -200,6 +208,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);
 int lists_build(Handle& h);
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
+int fmm_mixed_upward(Handle& h);   // upward pass on h.up, right after the tree (before the lists)
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);

@@ -272,20 +272,6 @@ __global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, uint3
     pbox[q] = b;
 }
 
-// flag the non-leaf boxes and count them per level
-__global__ void k_nonleaf_flags(int nb, const int* __restrict__ leafid, const int* __restrict__ level, int* flag,
-                                DevCounts* counts) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
-    const int f = leafid[b] < 0;
-    flag[b] = f;
-    if (f) atomicAdd(&counts->nonleaf_level[level[b]], 1);
-}
-
-__global__ void k_nonleaf_emit(int nb, const int* __restrict__ flag, const int64_t* __restrict__ off, int* out) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < nb && flag[b]) out[off[b]] = b;
-}
 
 inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
 inline int bits_for(int64_t v) {
@@ -324,24 +310,12 @@ int lists_build(Handle& h) {
                                                          nullptr, nullptr, dc); ++h.launches;
     OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
     OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
-    // non-leaf boxes in box order (level-major, so each level's parents are contiguous)
-    int *nl_flag, *nonleaf;
-    int64_t* nl_off;
-    OGX_TRY(arena_get(h.ws, S_NONLEAF_FLAG, nb, &nl_flag));
-    OGX_TRY(arena_get(h.ws, S_NONLEAF_OFF, nb + 1, &nl_off));
-    OGX_TRY(arena_get(h.ws, S_NONLEAF, nb, &nonleaf));
-    k_nonleaf_flags<<<grid_for(nb, 256), 256, 0, st>>>(nb, tv.leafid, tv.level, nl_flag, dc); ++h.launches;
-    OGX_TRY(scan_i32_to_i64(h, nl_flag, nl_off, nb));
-    k_nonleaf_emit<<<grid_for(nb, 256), 256, 0, st>>>(nb, nl_flag, nl_off, nonleaf); ++h.launches;
-    h.d_nonleaf = nonleaf;
     // sync point 2: list sizes
     OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaMemcpyAsync(&h.h_counts->u_total, uoff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaMemcpyAsync(&h.h_counts->w_total, woff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaStreamSynchronize(st));
     const int64_t nu = h.h_counts->u_total, nw = h.h_counts->w_total;
-    h.nonleaf_off.assign(h.max_level + 2, 0);
-    for (int l = 0; l <= h.max_level; ++l) h.nonleaf_off[l + 1] = h.nonleaf_off[l] + h.h_counts->nonleaf_level[l];
     int *uidx, *widx;
     OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
     OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));

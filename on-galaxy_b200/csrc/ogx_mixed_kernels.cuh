@@ -507,10 +507,11 @@ __device__ __forceinline__ double group_sum(double v, int tpg) {
 // of tpg = next power of two >= cnt lanes: lane (g, t) owns target body t and
 // takes every G-th source of each staged block, so small leaves keep most lanes
 // busy; the groups' partial sums (compensated per U entry) are combined in FP64
-// with shuffles.  Larger leaves run 32 targets at a time with G = 1.
+// with shuffles.  Larger leaves run 32 targets at a time with G = 1.  Output:
+// near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64; the kernel
+// needs only the tree and lists, so it runs beside the far-field chain.
 template <bool POT>
-__global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, double G, float eps2, const double* __restrict__ far,
-                                                    double* __restrict__ acc, double* __restrict__ pot) {
+__global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, float eps2, double* __restrict__ near) {
     __shared__ float4 s_hi[NEAR_STAGE], s_lo[NEAR_STAGE];
     const int lane = threadIdx.x & 31;
     const int lf = blockIdx.x;
@@ -558,13 +559,28 @@ __global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, double G, float
         const double nz = group_sum((double)sz - (double)cz, tpg);
         const double np = POT ? group_sum((double)sp - (double)cp, tpg) : 0.0;
         if (act && grp == 0) {
-            const int o = tv.perm[i];
-            acc[3 * (size_t)o] = G * (far[4 * (size_t)i] + nx);
-            acc[3 * (size_t)o + 1] = G * (far[4 * (size_t)i + 1] + ny);
-            acc[3 * (size_t)o + 2] = G * (far[4 * (size_t)i + 2] + nz);
-            if (POT) pot[o] = -G * (far[4 * (size_t)i + 3] + np);
+            double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)i);
+            o[0] = make_double2(nx, ny);
+            o[1] = make_double2(nz, np);
         }
     }
+}
+
+// acc[orig] = G (far + near), pot[orig] = -G (far + near) (AdaptiveFMM3D.hpp:104)
+template <bool POT>
+__global__ void k_combine(int n, const int* __restrict__ perm, double G, const double* __restrict__ far,
+                          const double* __restrict__ near, double* __restrict__ acc, double* __restrict__ pot) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int o = perm[i];
+    const double2 f0 = reinterpret_cast<const double2*>(far)[2 * (size_t)i];
+    const double2 f1 = reinterpret_cast<const double2*>(far)[2 * (size_t)i + 1];
+    const double2 n0 = reinterpret_cast<const double2*>(near)[2 * (size_t)i];
+    const double2 n1 = reinterpret_cast<const double2*>(near)[2 * (size_t)i + 1];
+    acc[3 * (size_t)o] = G * (f0.x + n0.x);
+    acc[3 * (size_t)o + 1] = G * (f0.y + n0.y);
+    acc[3 * (size_t)o + 2] = G * (f1.x + n1.x);
+    if (POT) pot[o] = -G * (f1.y + n1.y);
 }
 
 // ---- leaf far field in FP32 (L2P + W-list M2P) ----------------------------------------

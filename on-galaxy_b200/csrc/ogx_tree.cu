@@ -305,7 +305,34 @@ __global__ void k_gather_bodies(const uint32_t* perm, const double* pos, const d
 
 }  // namespace
 
-static inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
+static // flag the non-leaf boxes and count them per level
+__global__ void k_nonleaf_flags(int nb, const int* __restrict__ leafid, const int* __restrict__ level, int* flag,
+                                DevCounts* counts) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int f = leafid[b] < 0;
+    flag[b] = f;
+    if (f) atomicAdd(&counts->nonleaf_level[level[b]], 1);
+}
+
+__global__ void k_nonleaf_emit(int nb, const int* __restrict__ flag, const int64_t* __restrict__ off, int* out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nb && flag[b]) out[off[b]] = b;
+}
+
+// nl_off[l] = first non-leaf box of level l in the compacted list (exclusive scan of
+// the per-level counts; the list is level-major)
+__global__ void k_nonleaf_offsets(const DevCounts* counts, int* nl_off) {
+    if (threadIdx.x != 0) return;
+    int c = 0;
+    for (int l = 0; l <= kMaxDepth; ++l) {
+        nl_off[l] = c;
+        c += counts->nonleaf_level[l];
+    }
+    nl_off[kMaxDepth + 1] = c;
+}
+
+inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
 static inline int bits_for(int64_t v) {
     int b = 1;
     while ((1ll << b) <= v) ++b;
@@ -391,6 +418,21 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     k_boxes<<<grid_for(nb, 128), 128, 0, st>>>(nb, reclev, recpos_s, level_off_dev, khi, klo, leaflev, leafscan, leafstart, root,
                                                 level, coord, center, parent, child, leafid, pfirst, pcount, leafbox); ++h.launches;
     k_leaf_occupancy<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, pcount, dc); ++h.launches;
+
+    // non-leaf boxes in box order (level-major, so each level's parents are contiguous)
+    int *nl_flag, *nonleaf;
+    int64_t* nl_off;
+    OGX_TRY(arena_get(h.ws, S_NONLEAF_FLAG, nb, &nl_flag));
+    OGX_TRY(arena_get(h.ws, S_NONLEAF_OFF, nb + 1, &nl_off));
+    OGX_TRY(arena_get(h.ws, S_NONLEAF, nb, &nonleaf));
+    k_nonleaf_flags<<<grid_for(nb, 256), 256, 0, st>>>(nb, leafid, level, nl_flag, dc); ++h.launches;
+    OGX_TRY(scan_i32_to_i64(h, nl_flag, nl_off, nb));
+    k_nonleaf_emit<<<grid_for(nb, 256), 256, 0, st>>>(nb, nl_flag, nl_off, nonleaf); ++h.launches;
+    int* nl_loff;
+    OGX_TRY(arena_get(h.ws, S_NONLEAF_LOFF, kMaxDepth + 2, &nl_loff));
+    k_nonleaf_offsets<<<1, 32, 0, st>>>(dc, nl_loff); ++h.launches;
+    h.d_nonleaf = nonleaf;
+    h.d_nonleaf_off = nl_loff;
 
     // final body order: stable by leaf id from the original order
     uint32_t *lk, *ident;
