@@ -513,8 +513,9 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         const float eps2 = (float)(h.prm.eps * h.prm.eps);
         OGX_CUDA(cudaEventRecord(h.ev_fork, st));
         OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
-        if (d_pot) { mixed::k_leaf_near32<true><<<tv.nleaf, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
-        else { mixed::k_leaf_near32<false><<<tv.nleaf, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
+        const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
+        if (d_pot) { mixed::k_leaf_near32<true><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
+        else { mixed::k_leaf_near32<false><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
     if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }

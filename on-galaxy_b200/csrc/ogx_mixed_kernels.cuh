@@ -510,59 +510,62 @@ __device__ __forceinline__ double group_sum(double v, int tpg) {
 // with shuffles.  Larger leaves run 32 targets at a time with G = 1.  Output:
 // near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64; the kernel
 // needs only the tree and lists, so it runs beside the far-field chain.
+// Block b takes leaves b, b + gridDim.x, ... (one leaf per block at the usual
+// grid of one block per leaf).
 template <bool POT>
 __global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, float eps2, double* __restrict__ near) {
     __shared__ float4 s_hi[NEAR_STAGE], s_lo[NEAR_STAGE];
     const int lane = threadIdx.x & 31;
-    const int lf = blockIdx.x;
-    if (lf >= tv.nleaf) return;
-    const int b = tv.leafbox[lf];
-    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-    const double bcx = tv.center[4 * b], bcy = tv.center[4 * b + 1], bcz = tv.center[4 * b + 2];
-    const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
-    int tpg = 1;
-    while (tpg < min(cnt, 32)) tpg <<= 1;
-    const int ngrp = 32 / tpg, grp = lane / tpg, tl = lane & (tpg - 1);
-    for (int j0 = 0; j0 < cnt; j0 += tpg) {
-        const int jj = j0 + tl;
-        const bool act = jj < cnt;
-        const int i = f0 + (act ? jj : 0);
-        const double ddx = tv.px[i] - bcx, ddy = tv.py[i] - bcy, ddz = tv.pz[i] - bcz;
-        const float thx = (float)ddx, thy = (float)ddy, thz = (float)ddz;
-        const float tlx = (float)(ddx - (double)thx), tly = (float)(ddy - (double)thy), tlz = (float)(ddz - (double)thz);
-        float sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
-        for (int64_t e = u0; e < u1; ++e) {
-            const int c = tv.u_idx[e];
-            const int s0 = tv.pfirst[c], sc = tv.pcount[c];
-            float ax = 0, ay = 0, az = 0, ph = 0;
-            for (int k0 = 0; k0 < sc; k0 += NEAR_STAGE) {
-                const int n = min(NEAR_STAGE, sc - k0);
-                __syncwarp();
-                for (int q = lane; q < n; q += 32) {
-                    const int j = s0 + k0 + q;
-                    const double ex = tv.px[j] - bcx, ey = tv.py[j] - bcy, ez = tv.pz[j] - bcz;
-                    const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
-                    s_hi[q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
-                    s_lo[q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+    for (int lf = blockIdx.x; lf < tv.nleaf; lf += gridDim.x) {
+        const int b = tv.leafbox[lf];
+        const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+        const double bcx = tv.center[4 * b], bcy = tv.center[4 * b + 1], bcz = tv.center[4 * b + 2];
+        const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
+        int tpg = 1;
+        while (tpg < min(cnt, 32)) tpg <<= 1;
+        const int ngrp = 32 / tpg, grp = lane / tpg, tl = lane & (tpg - 1);
+        for (int j0 = 0; j0 < cnt; j0 += tpg) {
+            const int jj = j0 + tl;
+            const bool act = jj < cnt;
+            const int i = f0 + (act ? jj : 0);
+            const double ddx = tv.px[i] - bcx, ddy = tv.py[i] - bcy, ddz = tv.pz[i] - bcz;
+            const float thx = (float)ddx, thy = (float)ddy, thz = (float)ddz;
+            const float tlx = (float)(ddx - (double)thx), tly = (float)(ddy - (double)thy), tlz = (float)(ddz - (double)thz);
+            float sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
+            for (int64_t e = u0; e < u1; ++e) {
+                const int c = tv.u_idx[e];
+                const int s0 = tv.pfirst[c], sc = tv.pcount[c];
+                float ax = 0, ay = 0, az = 0, ph = 0;
+                for (int k0 = 0; k0 < sc; k0 += NEAR_STAGE) {
+                    const int n = min(NEAR_STAGE, sc - k0);
+                    __syncwarp();
+                    for (int q = lane; q < n; q += 32) {
+                        const int j = s0 + k0 + q;
+                        const double ex = tv.px[j] - bcx, ey = tv.py[j] - bcy, ez = tv.pz[j] - bcz;
+                        const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
+                        s_hi[q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
+                        s_lo[q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+                    }
+                    __syncwarp();
+                    if (c == b)
+                        p2p_block<true, POT>(s_hi, s_lo, grp, ngrp, n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+                    else
+                        p2p_block<false, POT>(s_hi, s_lo, grp, ngrp, n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
                 }
-                __syncwarp();
-                if (c == b)
-                    p2p_block<true, POT>(s_hi, s_lo, grp, ngrp, n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
-                else
-                    p2p_block<false, POT>(s_hi, s_lo, grp, ngrp, n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+                kahan_add(sx, cx, ax); kahan_add(sy, cy, ay); kahan_add(sz, cz, az);
+                if (POT) kahan_add(sp, cp, ph);
             }
-            kahan_add(sx, cx, ax); kahan_add(sy, cy, ay); kahan_add(sz, cz, az);
-            if (POT) kahan_add(sp, cp, ph);
+            const double nx = group_sum((double)sx - (double)cx, tpg);
+            const double ny = group_sum((double)sy - (double)cy, tpg);
+            const double nz = group_sum((double)sz - (double)cz, tpg);
+            const double np = POT ? group_sum((double)sp - (double)cp, tpg) : 0.0;
+            if (act && grp == 0) {
+                double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)i);
+                o[0] = make_double2(nx, ny);
+                o[1] = make_double2(nz, np);
+            }
         }
-        const double nx = group_sum((double)sx - (double)cx, tpg);
-        const double ny = group_sum((double)sy - (double)cy, tpg);
-        const double nz = group_sum((double)sz - (double)cz, tpg);
-        const double np = POT ? group_sum((double)sp - (double)cp, tpg) : 0.0;
-        if (act && grp == 0) {
-            double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)i);
-            o[0] = make_double2(nx, ny);
-            o[1] = make_double2(nz, np);
-        }
+        __syncwarp();
     }
 }
 
