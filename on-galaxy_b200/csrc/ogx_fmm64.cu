@@ -376,14 +376,6 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
 
 // ---- mixed form ---------------------------------------------------------------------
 // host emulation of cvt.rna.tf32.f32 (round to nearest, ties away from zero)
-inline float rna_tf32(float f) {
-    uint32_t u;
-    std::memcpy(&u, &f, 4);
-    u = (u + 0x1000u) & ~0x1FFFu;
-    float r;
-    std::memcpy(&r, &u, 4);
-    return r;
-}
 
 // Operator images for the tensor-core M2L, per offset o, K-chunk c and part (hi, lo):
 // rows = output dofs 1..K-1, K-major in the canonical no-swizzle core-matrix layout,
@@ -397,35 +389,48 @@ int ensure_mixed_tables(Handle& h) {
     std::vector<double> T((size_t)K * K);
     std::vector<uint8_t> img((size_t)343 * C::NCH * 2 * C::B_BYTES, 0);
     std::vector<double> row0((size_t)343 * K, 0.0);
+    std::vector<float> ounscale(343, 0.f);
     for (int o = 0; o < 343; ++o) {
         const int ox = o % 7 - 3, oy = (o / 7) % 7 - 3, oz = o / 49 - 3;
         if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) <= 1) continue;
         build_operator(2, P, o, T.data());
         for (int k = 0; k < K; ++k) row0[(size_t)o * K + k] = T[k];
+        // FP16 images of T_o * 2^-e, largest used entry in [0.5, 1); 2^e undoes it
+        double mx = 0.0;
+        for (int jr = 0; jr < C::N; ++jr)
+            for (int k = 0; k < K; ++k) mx = std::max(mx, std::fabs(T[(size_t)(jr + 1) * K + k]));
+        int e = 0;
+        if (mx > 0.0) std::frexp(mx, &e);
+        const double scale = std::ldexp(1.0, -e);
+        ounscale[o] = std::ldexp(1.0f, e);
         for (int c = 0; c < C::NCH; ++c) {
             uint8_t* hi = img.data() + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
             uint8_t* lo = hi + C::B_BYTES;
             for (int jr = 0; jr < C::N; ++jr)
-                for (int kk = 0; kk < C::CH * 8; ++kk) {
-                    const int k = c * C::CH * 8 + kk;
+                for (int kk = 0; kk < C::CH * 16; ++kk) {
+                    const int k = c * C::CH * 16 + kk;
                     if (k >= K) continue;
-                    const double x = T[(size_t)(jr + 1) * K + k];
-                    const float vh = rna_tf32((float)x);
-                    const float vl = rna_tf32((float)(x - (double)vh));
+                    const double x = T[(size_t)(jr + 1) * K + k] * scale;
+                    const __half vh = __double2half(x);
+                    const __half vl = __double2half(x - (double)__half2float(vh));
                     const int off = mixed::tile_off(jr, kk);
-                    std::memcpy(hi + off, &vh, 4);
-                    std::memcpy(lo + off, &vl, 4);
+                    std::memcpy(hi + off, &vh, 2);
+                    std::memcpy(lo + off, &vl, 2);
                 }
         }
     }
     uint8_t* d_img;
     double* d_row0;
+    float* d_ous;
     OGX_TRY(arena_get(h.ws, S_MIX_TOPS, img.size(), &d_img));
     OGX_TRY(arena_get(h.ws, S_MIX_ROW0, row0.size(), &d_row0));
+    OGX_TRY(arena_get(h.ws, S_MIX_OUNSCALE, ounscale.size(), &d_ous));
     OGX_CUDA(cudaMemcpy(d_img, img.data(), img.size(), cudaMemcpyHostToDevice));
     OGX_CUDA(cudaMemcpy(d_row0, row0.data(), row0.size() * sizeof(double), cudaMemcpyHostToDevice));
+    OGX_CUDA(cudaMemcpy(d_ous, ounscale.data(), ounscale.size() * sizeof(float), cudaMemcpyHostToDevice));
     h.d_tc_img = d_img;
     h.d_tc_row0 = d_row0;
+    h.d_tc_ounscale = d_ous;
     h.mix_ready_p = P;
     return OGX_OK;
 }
@@ -441,10 +446,12 @@ int run_mixed_upward(Handle& h) {
     OGX_TRY(harm_tables_ready(h.device));
     if constexpr (C::SUPPORTED) OGX_TRY(ensure_mixed_tables<P>(h));
     double* M;
-    float *mhi, *mlo;
+    __half *mhi, *mlo;
+    float* mus;
     OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
     OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
+    OGX_TRY(arena_get(h.ws, S_MIX_MUNSCALE, (size_t)tv.nb, &mus));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
     OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
     OGX_CUDA(cudaEventRecord(h.ev_tree, h.stream));
@@ -457,8 +464,7 @@ int run_mixed_upward(Handle& h) {
     h.stream = main_st;
     OGX_TRY(rc);
     if constexpr (C::SUPPORTED) {
-        const int64_t tot = (int64_t)tv.nb * C::KPAD;
-        mixed::k_split_mpole<P><<<(int)((tot + 255) / 256), 256, 0, su>>>(M, tv.nb, mhi, mlo); ++h.launches;
+        mixed::k_split_mpole<P><<<(tv.nb + 3) / 4, 128, 0, su>>>(M, tv.nb, mhi, mlo, mus); ++h.launches;
     }
     OGX_CUDA(cudaEventRecord(h.ev_up_end, su));
     OGX_CUDA(cudaEventRecord(h.ev_up, su));
@@ -473,13 +479,15 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     const cudaStream_t st = h.stream;
     TreeView& tv = h.tv;
     double *M, *L, *Lown, *far;
-    float *mhi, *mlo;
+    __half *mhi, *mlo;
+    float* mus;
     OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
     OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
     OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
     OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
     OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
+    OGX_TRY(arena_get(h.ws, S_MIX_MUNSCALE, (size_t)tv.nb, &mus));
     double* nearb;
     OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
@@ -492,8 +500,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     if (h.ntgt > 0) {
         if constexpr (C::SUPPORTED) {
             OGX_CUDA(cudaFuncSetAttribute(mixed::k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, mixed::TC_THREADS, C::SMEM, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, mhi,
-                                                                                 mlo, h.d_tc_img, Lown, h.d_err); ++h.launches;
+            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, mixed::TC_THREADS, C::SMEM, st>>>(
+                tv, h.tgt_tile_key, h.tgt_tile_box, mhi, mlo, mus, h.d_tc_img, h.d_tc_ounscale, Lown, h.d_err); ++h.launches;
             if (d_pot) {
                 mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, st>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,
                                                                              h.d_tc_row0, M, Lown); ++h.launches;

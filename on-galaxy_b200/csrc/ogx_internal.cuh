@@ -74,7 +74,7 @@ enum Slot {
     S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, S_TGT_TILE, S_TGT_PKEY, S_TGT_PBOX,
     S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
-    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
+    S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_MUNSCALE, S_MIX_OUNSCALE, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,
     S_NEAR32, S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
     S_NUM_SLOTS
@@ -182,6 +182,7 @@ struct Handle {
     int mix_ready_p = -1;
     uint8_t* d_tc_img = nullptr;   // tensor-core M2L operator images (hi/lo)
     double* d_tc_row0 = nullptr;   // row 0 of every M2L operator
+    float* d_tc_ounscale = nullptr; // per M2L operator: 2^e undoing the scaling of its FP16 images
     int* d_err = nullptr;          // device error word of the bounded waits
     int* h_err = nullptr;          // pinned copy
     // M2L targets (levels >= 2) sorted by child octant

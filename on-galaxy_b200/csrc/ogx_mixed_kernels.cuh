@@ -1,6 +1,6 @@
 // ogx_mixed_kernels.cuh -- kernels of the mixed-precision form.
 //
-// M2L on the 5th-generation tensor cores (tcgen05, kind::tf32, TMEM accumulators).
+// M2L on the 5th-generation tensor cores (tcgen05, kind::f16, TMEM accumulators).
 // The reference applies fmm::M2L pair by pair (src3d/FmmExpansions3D.hpp:273-299,
 // called per V-list entry in src3d/AdaptiveFMM3D.hpp:78-81).  Here:
 //   * a CTA owns 128 targets that share their octant t inside their parents
@@ -11,15 +11,20 @@
 //     most one source, so the sources of the 128 targets form the rows of a
 //     dense operand A (128 x K, zero rows where absent) and the translation is
 //     D[128 x N] = A . T_o^T with one operator matrix T_o for the whole tile;
-//   * split precision: multipoles and operators are split into TF32 hi + lo
-//     parts and D accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32
-//     (the dropped lo x lo term is ~2^-22 relative);
+//   * split precision: multipoles and operators are split into FP16 hi + lo
+//     parts (11 + 11 significant bits) and D accumulates A_hi B_hi + A_hi B_lo +
+//     A_lo B_hi in FP32 (the dropped lo x lo term is ~2^-22 relative).  FP16
+//     has the significand of TF32 at half the bytes, and the tensor cores' operand
+//     reads (shared memory) bound this kernel; its narrow exponent range is met by
+//     scaling every multipole row and every operator by a power of two that puts
+//     its largest entry in [0.5, 1), undone exactly per row and combination when
+//     the result is drained;
 //   * accumulation: FP32 accumulation over all ~6000 MMA steps of a tile loses
 //     ~1e-5 of the (strongly cancelling) far field, so every combination gets a
 //     fresh FP32 accumulator (two ping-pong buffers in TMEM) that the epilogue
 //     warps drain into an FP64 accumulator also kept in TMEM (two 32-bit
 //     columns per value) while the MMA warp proceeds with the next combination;
-//   * operands: K is cut into chunks of 32 tf32 (one 128-byte line per row) in
+//   * operands: K is cut into chunks of 64 fp16 (one 128-byte line per row) in
 //     the K-major 128-byte-swizzle layout; A rows are gathered with cp.async,
 //     each T_o chunk is a pre-laid-out image copied by the TMA bulk engine
 //     (cp.async.bulk, no multicast); up to 4 stages pipeline through mbarriers;
@@ -40,6 +45,8 @@
 // (Kahan) accumulator.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "ogx_harmonics.cuh"
 #include "ogx_sm100.cuh"
 
@@ -49,9 +56,9 @@ namespace mixed {
 template <int P>
 struct TcCfg {
     static constexpr int K = (P + 1) * (P + 1);
-    static constexpr int KPAD = (K + 7) / 8 * 8;
-    static constexpr int NKS = KPAD / 8;      // K-steps of the MMA (8 tf32 each)
-    static constexpr int CH = 4;              // K-steps per pipeline chunk
+    static constexpr int KPAD = (K + 15) / 16 * 16;
+    static constexpr int NKS = KPAD / 16;     // K-steps of the MMA (16 fp16 each)
+    static constexpr int CH = 4;              // K-steps per pipeline chunk (64 fp16 = one 128-byte line)
     static constexpr int NCH = (NKS + CH - 1) / CH;
     static constexpr int N = K - 1;           // output dofs 1..K-1
     static constexpr int NPAD = (N + 15) / 16 * 16;
@@ -71,16 +78,16 @@ struct TcCfg {
     static constexpr int ACC64 = 2 * DBUF;    // first column of the FP64 accumulator
     static constexpr int TMEM_COLS = 512;
     static constexpr bool SUPPORTED = 4 * NPAD <= 512 && STAGES >= 2;
-    static_assert(CH * 8 * 4 == 128, "a chunk row must fill exactly one 128-byte swizzle line");
+    static_assert(CH * 16 * 2 == 128, "a chunk row must fill exactly one 128-byte swizzle line");
 };
 
-// Byte offset of element (row, kk), kk < 32, inside one operand of a stage, in the
-// K-major 128-byte-swizzle layout: each row's 32 tf32 of the chunk fill one
-// 128-byte line, 8 rows form a 1024-byte atom, and 16-byte piece j of row r sits
-// at piece position j ^ (r mod 8) so the tensor core reads the 8 rows of an atom
-// from different banks.  Operand bases are 1024-byte aligned.
+// Byte offset of fp16 element (row, kk), kk < 64, inside one operand of a stage,
+// in the K-major 128-byte-swizzle layout: each row's 64 fp16 of the chunk fill
+// one 128-byte line, 8 rows form a 1024-byte atom, and 16-byte piece j of row r
+// sits at piece position j ^ (r mod 8) so the tensor core reads the 8 rows of an
+// atom from different banks.  Operand bases are 1024-byte aligned.
 __host__ __device__ __forceinline__ int tile_off(int row, int kk) {
-    return (row >> 3) * 1024 + (row & 7) * 128 + ((((kk >> 2) ^ row) & 7) << 4) + (kk & 3) * 4;
+    return (row >> 3) * 1024 + (row & 7) * 128 + ((((kk >> 3) ^ row) & 7) << 4) + (kk & 7) * 2;
 }
 
 // Warp roles: warps 0-3 gather the A rows (thread r owns target row r), warp 4
@@ -103,9 +110,10 @@ __device__ __forceinline__ void tmem_st_wait() { asm volatile("tcgen05.wait::st.
 
 // Add the FP32 combination result in D buffer `a` (16-column groups g0..g1-1) to
 // the FP64 accumulator of this warp's 32 lanes; `first` initialises it instead.
-// PAIR: the buffer holds two partial products NPAD columns apart.
+// PAIR: the buffer holds two partial products NPAD columns apart.  `unscale`
+// (a power of two) undoes the row's source scale and the operator's scale.
 template <int NPAD, int DBUF, int ACC64, bool PAIR>
-__device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first, int g0, int g1) {
+__device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool first, int g0, int g1, float unscale) {
 #pragma unroll 1
     for (int c16 = g0; c16 < g1; ++c16) {
         uint32_t v[16], w[16], lo[16], hi[16];
@@ -118,8 +126,8 @@ __device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool firs
         sm100::tmem_ld_wait();
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-            double s = (double)__uint_as_float(v[k]);
-            if (PAIR) s += (double)__uint_as_float(w[k]);
+            double s = (double)(__uint_as_float(v[k]) * unscale);
+            if (PAIR) s += (double)(__uint_as_float(w[k]) * unscale);
             if (!first) s += __hiloint2double((int)hi[k], (int)lo[k]);
             lo[k] = (uint32_t)__double2loint(s);
             hi[k] = (uint32_t)__double2hiint(s);
@@ -133,8 +141,8 @@ __device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool firs
 template <int P>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_m2l_tc(TreeView tv, const uint32_t* __restrict__ tgt_key, const uint32_t* __restrict__ tgt_box,
-             const float* __restrict__ mhi, const float* __restrict__ mlo, const uint8_t* __restrict__ btab,
-             double* __restrict__ lown, int* err) {
+             const __half* __restrict__ mhi, const __half* __restrict__ mlo, const float* __restrict__ munscale,
+             const uint8_t* __restrict__ btab, const float* __restrict__ ounscale, double* __restrict__ lown, int* err) {
     using C = TcCfg<P>;
     static_assert(C::SUPPORTED, "tensor-core M2L serves p <= 10");
     // gathers kept in flight per producer thread before its row is handed to the MMA
@@ -233,8 +241,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 4) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            constexpr uint32_t idesc = sm100::idesc_tf32(C::M, C::NPAD);
-            constexpr uint32_t idesc2 = sm100::idesc_tf32(C::M, 2 * C::NPAD);
+            constexpr uint32_t idesc = sm100::idesc_f16(C::M, C::NPAD);
+            constexpr uint32_t idesc2 = sm100::idesc_f16(C::M, 2 * C::NPAD);
             // descriptors differ only in their 14-bit start-address field (bytes >> 4):
             // build stage 0's once and add the stage / K-step / operand offsets
             const uint64_t desc0 = sm100::smem_desc_sw128(sm100::smem_u32(smem), C::SBO);
@@ -269,14 +277,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         if (ks < nks) {
                             const uint64_t dk = ds + (uint64_t)(ks * 2);    // 32 bytes per K-step inside the line
                             if constexpr (C::PAIR) {
-                                sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc2, accum);      // A_hi x [B_hi | B_lo]
+                                sm100::mma_f16(dcol, dk, dk + D_BHI, idesc2, accum);      // A_hi x [B_hi | B_lo]
                                 accum = 1;
-                                sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);    // A_lo x B_hi
+                                sm100::mma_f16(dcol, dk + D_LO, dk + D_BHI, idesc, 1);    // A_lo x B_hi
                             } else {
-                                sm100::mma_tf32(dcol, dk, dk + D_BHI, idesc, accum);
+                                sm100::mma_f16(dcol, dk, dk + D_BHI, idesc, accum);
                                 accum = 1;
-                                sm100::mma_tf32(dcol, dk, dk + D_BLO, idesc, 1);
-                                sm100::mma_tf32(dcol, dk + D_LO, dk + D_BHI, idesc, 1);
+                                sm100::mma_f16(dcol, dk, dk + D_BLO, idesc, 1);
+                                sm100::mma_f16(dcol, dk + D_LO, dk + D_BHI, idesc, 1);
                             }
                         }
                     }
@@ -336,17 +344,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 // the warp copies its 32 rows cooperatively: one instruction moves
                 // 16-byte pieces q0..q0+3 of 8 rows, so each source row is read in
                 // whole 64-byte runs and a quarter-warp fills 8 consecutive slots
-                const int k0 = c * C::CH * 8;
-                const int nq = min(2 * C::CH, (C::KPAD - k0) / 4);
+                const int k0 = c * C::CH * 16;
+                const int nq = min(8, (C::KPAD - k0) / 8);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     const int rl = 8 * (i >> 2) + (lane & 7);         // row within the warp
                     const int part = (i >> 1) & 1;                    // 0: hi, 1: lo
-                    const int q = (i & 1) * 4 + (lane >> 3);          // 16-byte piece of the chunk
+                    const int q = (i & 1) * 4 + (lane >> 3);          // 16-byte piece (8 fp16) of the chunk
                     const int rs = __shfl_sync(0xffffffffu, src, rl);
                     if (q < nq) {
-                        const float* g = (part ? mlo : mhi) + (size_t)max(rs, 0) * C::KPAD + k0 + 4 * q;
-                        sm100::cp_async16_zfill(st + part * C::A_BYTES + tile_off(32 * warp + rl, 4 * q), g,
+                        const __half* g = (part ? mlo : mhi) + (size_t)max(rs, 0) * C::KPAD + k0 + 8 * q;
+                        sm100::cp_async16_zfill(st + part * C::A_BYTES + tile_off(32 * warp + rl, 8 * q), g,
                                                 rs >= 0 ? 16u : 0u);
                     }
                 }
@@ -373,15 +381,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int grp = (warp - 5) >> 2;              // column slice of this warp
         const int g0 = grp * NG / NGRP, g1 = (grp + 1) * NG / NGRP;
         const uint32_t tmem_lane = tmem + ((uint32_t)(quarter * 32) << 16);
+        const int row = quarter * 32 + lane;
         for (int k = 0; k < nco && !s_abort; ++k) {
             const int a = k & 1;
+            // this row's source for combination k and the scales its operands carry
+            const int code = s_combo[k];
+            const int Q = s_Q[code & 31][row];
+            const int srcb = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((code >> 5) & 7)) : -1;
+            const float unscale = (srcb >= 0) ? __ldg(munscale + srcb) * __ldg(ounscale + (code >> 8)) : 0.f;
             if (!sm100::mbar_wait(&dfull[a], (k >> 1) & 1, &s_abort)) {
                 s_abort = 1;
                 atomicExch(err, 1);
                 break;
             }
             sm100::tc_fence_after();
-            drain_combo<C::NPAD, C::DBUF, C::ACC64, C::PAIR>(tmem_lane, a, k == 0, g0, g1);
+            drain_combo<C::NPAD, C::DBUF, C::ACC64, C::PAIR>(tmem_lane, a, k == 0, g0, g1, unscale);
             sm100::tc_fence_before();
             sm100::mbar_arrive(&dempty[a]);
         }
@@ -414,18 +428,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
 }
 
-// FP64 multipoles -> TF32 hi/lo pairs, rows padded to KPAD with zeros
+// FP64 multipoles -> scaled FP16 hi/lo pairs, rows padded to KPAD with zeros.  Warp
+// per box: the row is scaled by a power of two 2^-e so that its largest entry lies
+// in [0.5, 1) (FP16 keeps 11 significant bits like TF32 but has a narrow exponent
+// range); hi = fp16(x), lo = fp16(x - hi); munscale[b] = 2^e undoes the scaling
+// exactly when the M2L result is drained.
 template <int P>
-__global__ void k_split_mpole(const double* __restrict__ M, int nb, float* __restrict__ hi, float* __restrict__ lo) {
+__global__ void __launch_bounds__(128) k_split_mpole(const double* __restrict__ M, int nb, __half* __restrict__ hi,
+                                                     __half* __restrict__ lo, float* __restrict__ munscale) {
     using C = TcCfg<P>;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= (int64_t)nb * C::KPAD) return;
-    const int64_t b = i / C::KPAD;
-    const int k = (int)(i - b * C::KPAD);
-    const double x = (k < C::K) ? M[b * C::K + k] : 0.0;
-    const float h = sm100::to_tf32((float)x);
-    hi[i] = h;
-    lo[i] = sm100::to_tf32((float)(x - (double)h));
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (b >= nb) return;
+    const double* row = M + (size_t)b * C::K;
+    double mx = 0.0;
+    for (int k = lane; k < C::K; k += 32) mx = fmax(mx, fabs(row[k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);
+    const double scale = ldexp(1.0, -e);
+    for (int k = lane; k < C::KPAD; k += 32) {
+        const double x = (k < C::K) ? row[k] * scale : 0.0;
+        const __half h = __double2half(x);
+        hi[(size_t)b * C::KPAD + k] = h;
+        lo[(size_t)b * C::KPAD + k] = __double2half(x - (double)__half2float(h));
+    }
+    if (lane == 0) munscale[b] = ldexpf(1.0f, e);
 }
 
 // L_0^0 of the M2L (needed only for potentials): FP64 row 0 of every T_o
