@@ -48,6 +48,9 @@ inline double ref_dm_S(int n, int m) { return ((m > 0) ? 1.0 : -1.0) * std::sqrt
 // One copy per translation unit (whole-program compilation, no device linking);
 // every unit that launches harmonic kernels calls harm_tables_ready() first.
 static __constant__ HarmTables c_harm;
+// the same tables in global memory, for kernels whose lanes index them divergently
+// (the constant cache serialises lanes that read different addresses)
+static __device__ HarmTables g_harm;
 
 static inline void fill_harm_tables(HarmTables& t) {
     t = HarmTables{};
@@ -85,7 +88,8 @@ static inline int harm_tables_ready(int device) {
     if (done[device]) return OGX_OK;
     HarmTables t;
     fill_harm_tables(t);
-    const cudaError_t e = cudaMemcpyToSymbol(c_harm, &t, sizeof(t));
+    cudaError_t e = cudaMemcpyToSymbol(c_harm, &t, sizeof(t));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_harm, &t, sizeof(t));
     if (e != cudaSuccess) {
         set_last_error(OGX_ERR_CUDA, std::string("harmonic tables: ") + cudaGetErrorString(e));
         return OGX_ERR_CUDA;

@@ -630,6 +630,28 @@ struct FarRec32 {
     static constexpr int NEG = (P + 1) * (P + 2) / 2;   // entries of an L2P record
 };
 
+// Both parts (re, im) of entry (n, m) of a gradient coefficient set, the values
+// mpole_grad_dof / local_grad_dof give for dofs dof_re(n, m) and dof_re(n, m) + 1,
+// with the constants read from global memory (lanes hold different (n, m)).
+//   MODE 0: multipole set H from M_{n-1} (dz_S / dp_S / dm_S, FmmExpansions3D.hpp:121-129)
+//   MODE 1: local set G from L_{n+1}    (cz_R / cp_R / cm_R, FmmExpansions3D.hpp:111-119)
+template <int MODE>
+__device__ __forceinline__ void grad_entry(const double* c, int n, int m, float gr[3], float gi[3]) {
+    if (MODE == 0 && n == 0) return;
+    const int N = MODE == 0 ? n - 1 : n + 1;
+    double lr, li, pr, pi, mr, mi;
+    coef_get(c, N, m, lr, li);
+    coef_get(c, N, m - 1, mr, mi);
+    coef_get(c, N, m + 1, pr, pi);
+    const double cz = __ldg(MODE == 0 ? &g_harm.hz[n][m] : &g_harm.gz[n][m]);
+    const double cp = __ldg(MODE == 0 ? &g_harm.hp[n][m] : &g_harm.gp[n][m]);
+    const double cm = __ldg(MODE == 0 ? &g_harm.hm[n][m] : &g_harm.gm[n][m]);
+    const double xr = 0.5 * (cp * mr + cm * pr), xi = 0.5 * (cp * mi + cm * pi);
+    const double dr = cp * mr - cm * pr, di = cp * mi - cm * pi;
+    gr[0] = (float)xr; gr[1] = (float)(0.5 * di); gr[2] = (float)(cz * lr);
+    if (m > 0) { gi[0] = (float)xi; gi[1] = (float)(-0.5 * dr); gi[2] = (float)(cz * li); }
+}
+
 template <int P, int MODE>
 __global__ void __launch_bounds__(128) k_far_rec32(TreeView tv, int count, const double* __restrict__ coef,
                                                    float4* __restrict__ rec) {
@@ -649,13 +671,7 @@ __global__ void __launch_bounds__(128) k_far_rec32(TreeView tv, int count, const
         const int dr = dof_re(n, m);
         float gr[3] = {0.f, 0.f, 0.f}, gi[3] = {0.f, 0.f, 0.f};
         float pr = 0.f, pi = 0.f;
-        if (MODE == 0) {
-            mpole_grad_dof(c, dr, gr);
-            if (m > 0) mpole_grad_dof(c, dr + 1, gi);
-        } else if (n < P) {
-            local_grad_dof(c, dr, gr);
-            if (m > 0) local_grad_dof(c, dr + 1, gi);
-        }
+        if (MODE == 0 || n < P) grad_entry<MODE>(c, n, m, gr, gi);
         if (n <= P) {
             pr = (float)c[dr];
             if (m > 0) pi = (float)c[dr + 1];
@@ -852,7 +868,7 @@ __global__ void k_far_heavy_list(TreeView tv, int* __restrict__ list, int* count
 // warp 0 also the L2P; the warps' per-body partial sums are added in warp order
 // through shared memory (deterministic).
 template <int P, bool POT>
-__global__ void __launch_bounds__(32 * FAR_HW) k_leaf_far32_heavy(TreeView tv, const float4* __restrict__ hrec,
+__global__ void __launch_bounds__(32 * FAR_HW, 3) k_leaf_far32_heavy(TreeView tv, const float4* __restrict__ hrec,
                                                                  const float4* __restrict__ grec, double* __restrict__ far,
                                                                  const int* __restrict__ list, int* ctr) {
     constexpr int NEG = FarRec32<P>::NEG;
