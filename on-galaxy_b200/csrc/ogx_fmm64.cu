@@ -83,13 +83,16 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
 }
 
 // ---- M2M (MODE 0) / L2L (MODE 1) over the non-leaf parents of one level ------------
-// CTA = TR_PB parents x 8 warps, warp s = child octant s.  Warp s applies the
+// CTA = tr_pb<P>() parents x 8 warps, warp s = child octant s.  Warp s applies the
 // operator MM_s / LL_s (transposed, k-major, L2-resident) to its TR_PB parents,
 // lanes over output dofs.
 //   M2M: M'_P = sum_s MM_s M'_{child s}                (src3d/AdaptiveFMM3D.hpp:62-71)
 //        the eight partial products are summed in octant order through shared memory
 //   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
-constexpr int TR_PB = 2;   // parents per CTA
+// parents per CTA: each warp applies its operator to TR_PB parents per load of an
+// operator row (4 where the shared staging fits the 48 KB static limit)
+template <int P>
+constexpr int tr_pb() { return (P + 1) * (P + 1) <= 81 ? 4 : 2; }
 template <int P, int MODE>
 __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* __restrict__ nonleaf,
                                                        const int* __restrict__ nl_off, int level,
@@ -97,6 +100,7 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
                                                        const double* __restrict__ lown) {
     constexpr int K = (P + 1) * (P + 1);
     constexpr int NPL = (K + 31) / 32;
+    constexpr int TR_PB = tr_pb<P>();
     __shared__ double s_in[MODE == 0 ? 8 : 1][TR_PB][K];
     __shared__ double s_part[MODE == 0 ? 8 : 1][TR_PB][MODE == 0 ? K : 1];
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
@@ -185,7 +189,7 @@ template <int P>
 int launch_m2m(Handle& h, double* M) {
     for (int l = h.max_level - 1; l >= 0; --l) {
         const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
-        if (nbl > 0) { k_translate_oct<P, 0><<<(nbl + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+        if (nbl > 0) { k_translate_oct<P, 0><<<(nbl + tr_pb<P>() - 1) / tr_pb<P>(), 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -198,7 +202,7 @@ int launch_l2l(Handle& h, double* L, const double* Lown) {
                              cudaMemcpyDeviceToDevice, h.stream));
     for (int l = 0; l < h.max_level; ++l) {
         const int nbl = h.level_off[l + 1] - h.level_off[l];
-        if (nbl > 0) { k_translate_oct<P, 1><<<(nbl + TR_PB - 1) / TR_PB, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+        if (nbl > 0) { k_translate_oct<P, 1><<<(nbl + tr_pb<P>() - 1) / tr_pb<P>(), 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
     }
     return OGX_OK;
 }
