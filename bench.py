@@ -47,7 +47,7 @@ DT = 0.01
 # dram__bytes_write.sum of k_m2l_tc<8> divided by the launch's V-list pairs), from the
 # ncu capture summarised in profiles/k_m2l_tc_merger500k.md; the bytes scale with the
 # pairs a launch processes (sources gathered per pair, results per target).
-M2L_DRAM_BYTES_PER_VPAIR = 22.16
+M2L_DRAM_BYTES_PER_VPAIR = 15.13
 
 
 def arm_config(n, n_per, world):
@@ -333,7 +333,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "mixed(f32 P2P, 3xTF32 M2L, f64 translations)" if prec == ogx.PREC_MIXED else "f64",
+        "vs_baseline": None, "dtype": "mixed(f32 P2P, scaled 3xFP16 tensor-core M2L, f64 translations)" if prec == ogx.PREC_MIXED else "f64",
         "data": "synthetic",
         "config": arm_config(n, args.n_per, world),
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
