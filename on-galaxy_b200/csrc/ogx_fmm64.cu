@@ -504,7 +504,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     if (h.ntgt > 0) {
         if constexpr (C::SUPPORTED) {
             OGX_CUDA(cudaFuncSetAttribute(mixed::k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, mixed::TC_THREADS, C::SMEM, st>>>(
+            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, C::THREADS, C::SMEM, st>>>(
                 tv, h.tgt_tile_key, h.tgt_tile_box, mhi, mlo, mus, h.d_tc_img, h.d_tc_ounscale, Lown, h.d_err); ++h.launches;
             if (d_pot) {
                 mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, st>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,

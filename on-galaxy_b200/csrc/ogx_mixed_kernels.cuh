@@ -75,7 +75,18 @@ struct TcCfg {
     // A combination buffer then holds [hh + lh | hl], summed when drained.
     static constexpr bool PAIR = 6 * NPAD <= 512;
     static constexpr int DBUF = PAIR ? 2 * NPAD : NPAD;  // TMEM columns of one FP32 buffer
-    static constexpr int ACC64 = 2 * DBUF;    // first column of the FP64 accumulator
+    // REGACC (p <= 8): one group of four drain warps per 16-column slice of the
+    // output, each lane keeping its 16 FP64 sums in registers (a combination costs a
+    // drain warp one TMEM load round trip); TMEM then holds only FP32 buffers, NBUF
+    // of them in a ring, so the MMA runs NBUF - 1 combinations ahead of the drain.
+    // Otherwise two column slices, FP64 sums in TMEM at column ACC64, two buffers.
+    static constexpr bool REGACC = PAIR;
+    static constexpr int NGRP = REGACC ? NPAD / 16 : 2;  // column slices
+    static constexpr int MAXG = (NPAD / 16 + NGRP - 1) / NGRP;
+    static constexpr int DRAIN_WARPS = 4 * NGRP;
+    static constexpr int THREADS = 128 + 32 + 32 * DRAIN_WARPS;   // producers, MMA warp, drain warps
+    static constexpr int NBUF = REGACC ? 512 / DBUF : 2;
+    static constexpr int ACC64 = 2 * DBUF;    // first column of the FP64 accumulator (TMEM form)
     static constexpr int TMEM_COLS = 512;
     static constexpr bool SUPPORTED = 4 * NPAD <= 512 && STAGES >= 2;
     static_assert(CH * 16 * 2 == 128, "a chunk row must fill exactly one 128-byte swizzle line");
@@ -91,13 +102,11 @@ __host__ __device__ __forceinline__ int tile_off(int row, int kk) {
 }
 
 // Warp roles: warps 0-3 gather the A rows (thread r owns target row r), warp 4
-// issues the MMAs (one lane), warps 5..5+TC_DRAIN_WARPS-1 fold every combination's
-// FP32 result into the FP64 accumulator and write the tile's result.  A warp may
-// only touch the TMEM lane quarter (warp index mod 4), so the drain warps come in
-// groups of four, each group owning a slice of the output columns.
+// issues the MMAs (one lane), warps 5..5+TcCfg::DRAIN_WARPS-1 fold every
+// combination's FP32 result into the FP64 accumulator and write the tile's result.
+// A warp may only touch the TMEM lane quarter (warp index mod 4), so the drain warps
+// come in groups of four, each group owning a slice of the output columns.
 constexpr int TC_PRODUCERS = 128;
-constexpr int TC_DRAIN_WARPS = 8;
-constexpr int TC_THREADS = TC_PRODUCERS + 32 + 32 * TC_DRAIN_WARPS;
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(
@@ -139,7 +148,7 @@ __device__ __forceinline__ void drain_combo(uint32_t tmem_lane, int a, bool firs
 }
 
 template <int P>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
     k_m2l_tc(TreeView tv, const uint32_t* __restrict__ tgt_key, const uint32_t* __restrict__ tgt_box,
              const __half* __restrict__ mhi, const __half* __restrict__ mlo, const float* __restrict__ munscale,
              const uint8_t* __restrict__ btab, const float* __restrict__ ounscale, double* __restrict__ lown, int* err) {
@@ -148,10 +157,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // gathers kept in flight per producer thread before its row is handed to the MMA
     constexpr int LAG = C::STAGES >= 4 ? C::STAGES - 2 : 1;
     constexpr int NG = C::NPAD / 16;
-    constexpr int NGRP = TC_DRAIN_WARPS / 4;
+    constexpr int NGRP = C::NGRP;
+    constexpr int NBUF = C::NBUF;
+    static_assert(NBUF * C::DBUF + (C::REGACC ? 0 : 2 * C::NPAD) <= C::TMEM_COLS, "TMEM budget");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    __shared__ uint64_t afull[C::STAGES], bfull[C::STAGES], empty[C::STAGES], dfull[2], dempty[2], fin;
+    __shared__ uint64_t afull[C::STAGES], bfull[C::STAGES], empty[C::STAGES], dfull[C::NBUF], dempty[C::NBUF], fin;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ int s_t, s_ncombo;
@@ -169,9 +180,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             sm100::mbar_init(&bfull[s], 1);
             sm100::mbar_init(&empty[s], 1);
         }
-        for (int a = 0; a < 2; ++a) {
+        for (int a = 0; a < C::NBUF; ++a) {
             sm100::mbar_init(&dfull[a], 1);
-            sm100::mbar_init(&dempty[a], 32 * TC_DRAIN_WARPS);
+            sm100::mbar_init(&dempty[a], 32 * C::DRAIN_WARPS);
         }
         sm100::mbar_init(&fin, 1);
         sm100::fence_mbar_init();
@@ -250,9 +261,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                D_BLO = (2 * C::A_BYTES + C::B_BYTES) >> 4, D_STAGE = C::STAGE_BYTES >> 4;
             int u = 0;
             for (int k = 0; k < nco && !s_abort; ++k) {
-                const int a = k & 1;
-                if (k >= 2) {
-                    if (!sm100::mbar_wait(&dempty[a], ((k >> 1) - 1) & 1, &s_abort)) {
+                const int a = k % NBUF;
+                if (k >= NBUF) {
+                    if (!sm100::mbar_wait(&dempty[a], ((k / NBUF) - 1) & 1, &s_abort)) {
                         s_abort = 1;
                         atomicExch(err, 1);
                         break;
@@ -382,38 +393,78 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int g0 = grp * NG / NGRP, g1 = (grp + 1) * NG / NGRP;
         const uint32_t tmem_lane = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;
+        double racc[C::REGACC ? C::MAXG : 1][16];
+#pragma unroll
+        for (int g = 0; g < (C::REGACC ? C::MAXG : 1); ++g)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) racc[g][i] = 0.0;
         for (int k = 0; k < nco && !s_abort; ++k) {
-            const int a = k & 1;
+            const int a = k % NBUF;
             // this row's source for combination k and the scales its operands carry
             const int code = s_combo[k];
             const int Q = s_Q[code & 31][row];
             const int srcb = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((code >> 5) & 7)) : -1;
             const float unscale = (srcb >= 0) ? __ldg(munscale + srcb) * __ldg(ounscale + (code >> 8)) : 0.f;
-            if (!sm100::mbar_wait(&dfull[a], (k >> 1) & 1, &s_abort)) {
+            if (!sm100::mbar_wait(&dfull[a], (k / NBUF) & 1, &s_abort)) {
                 s_abort = 1;
                 atomicExch(err, 1);
                 break;
             }
             sm100::tc_fence_after();
-            drain_combo<C::NPAD, C::DBUF, C::ACC64, C::PAIR>(tmem_lane, a, k == 0, g0, g1, unscale);
+            if constexpr (C::REGACC) {
+#pragma unroll
+                for (int g = 0; g < C::MAXG; ++g) {
+                    const int c16 = g0 + g;
+                    if (c16 < g1) {
+                        uint32_t v[16], w[16];
+                        sm100::tmem_ld16(tmem_lane + a * C::DBUF + c16 * 16, v);
+                        sm100::tmem_ld16(tmem_lane + a * C::DBUF + C::NPAD + c16 * 16, w);
+                        sm100::tmem_ld_wait();
+                        // the two partial products meet in FP32 (w is ~2^-11 of v), then one
+                        // conversion and one FP64 add per column: the FP64 pipe bounds the drain
+#pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                            racc[g][i] += (double)((__uint_as_float(v[i]) + __uint_as_float(w[i])) * unscale);
+                    }
+                }
+            } else {
+                drain_combo<C::NPAD, C::DBUF, C::ACC64, C::PAIR>(tmem_lane, a, k == 0, g0, g1, unscale);
+            }
             sm100::tc_fence_before();
             sm100::mbar_arrive(&dempty[a]);
         }
         if (nco >= 1 && !s_abort) {
             const int myb = s_box[quarter * 32 + lane];
             const double inv = (myb >= 0) ? 1.0 / (2.0 * tv.center[4 * myb + 3]) : 0.0;
-#pragma unroll 1
-            for (int c16 = g0; c16 < g1; ++c16) {
-                uint32_t lo[16], hi[16];
-                sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32, lo);
-                sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32 + 16, hi);
-                sm100::tmem_ld_wait();
+            if constexpr (C::REGACC) {
                 if (myb >= 0) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int dof = 1 + c16 * 16 + k;
-                        if (dof < C::K)
-                            lown[(size_t)myb * C::K + dof] += __hiloint2double((int)hi[k], (int)lo[k]) * inv;
+                    for (int g = 0; g < C::MAXG; ++g) {
+                        const int c16 = g0 + g;
+                        if (c16 < g1) {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) {
+                                const int dof = 1 + c16 * 16 + i;
+                                if (dof < C::K) lown[(size_t)myb * C::K + dof] += racc[g][i] * inv;
+                            }
+                        }
+                    }
+                }
+            } else {
+                sm100::tc_fence_after();
+#pragma unroll 1
+                for (int c16 = g0; c16 < g1; ++c16) {
+                    uint32_t lo[16], hi[16];
+                    sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32, lo);
+                    sm100::tmem_ld16(tmem_lane + C::ACC64 + c16 * 32 + 16, hi);
+                    sm100::tmem_ld_wait();
+                    if (myb >= 0) {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            const int dof = 1 + c16 * 16 + k;
+                            if (dof < C::K)
+                                lown[(size_t)myb * C::K + dof] += __hiloint2double((int)hi[k], (int)lo[k]) * inv;
+                        }
                     }
                 }
             }
