@@ -119,6 +119,8 @@ struct DevCounts {
     int32_t kernel_error;  // set by kernels whose bounded waits ran out
     int32_t pad_err;
     int32_t nonleaf_level[kMaxDepth + 2];
+    int32_t deep_flag;   // some level-16 box holds more than leaf_capacity bodies
+    int32_t pad_deep;
 };
 
 // device view of the tree handed to kernels
@@ -221,7 +223,9 @@ int direct_launch(const double* d_pos, const double* d_mass, int64_t n, double G
 // generic radix sort helpers (ogx_sort.cu)
 int radix_sort_u32(Handle& h, Slot kin, Slot vin, Slot kalt, Slot valt, int64_t n, int bits,
                    uint32_t** kout, uint32_t** vout);
-int radix_sort_key72(Handle& h, int64_t n, uint64_t** khi, uint32_t** klo, uint32_t** idx);
+// stable LSD sort of the 72-bit keys over digit passes first_pass..8 (first_pass 3 orders
+// by levels 1..16 only)
+int radix_sort_key72(Handle& h, int64_t n, int first_pass, uint64_t** khi, uint32_t** klo, uint32_t** idx);
 int scan_i32_to_i64(Handle& h, const int* in, int64_t* out, int64_t n);  // exclusive, out[n] = total
 
 }  // namespace ogx

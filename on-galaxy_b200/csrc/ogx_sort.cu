@@ -275,14 +275,15 @@ int scan_i32_to_i64(Handle& h, const int* in, int64_t* out, int64_t n) {
 }
 
 template <class KO>
-static int radix_passes(Handle& h, KO a, KO b, uint32_t* va, uint32_t* vb, int64_t n, int npasses, int* which) {
+static int radix_passes(Handle& h, KO a, KO b, uint32_t* va, uint32_t* vb, int64_t n, int npasses, int* which,
+                        int first_pass = 0) {
     const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
     uint32_t* hist;
     OGX_TRY(arena_get(h.ws, S_RS_HIST, (size_t)256 * nblocks + 256, &hist));
     uint32_t* tot = hist + (size_t)256 * nblocks;
     KO src = a, dst = b;
     uint32_t *vs = va, *vd = vb;
-    for (int pass = 0; pass < npasses; ++pass) {
+    for (int pass = first_pass; pass < npasses; ++pass) {
         rs_hist<KO><<<nblocks, RS_THREADS, 0, h.stream>>>(src, n, pass, hist, nblocks); ++h.launches;
         rs_scan_digit<<<256, 1024, 0, h.stream>>>(hist, nblocks, tot); ++h.launches;
         rs_scan_totals<<<1, 256, 0, h.stream>>>(tot); ++h.launches;
@@ -291,7 +292,7 @@ static int radix_passes(Handle& h, KO a, KO b, uint32_t* va, uint32_t* vb, int64
         std::swap(vs, vd);
     }
     OGX_CUDA(cudaGetLastError());
-    *which = npasses & 1;  // 0: result in a, 1: result in b
+    *which = (npasses - first_pass) & 1;  // 0: result in a, 1: result in b
     return OGX_OK;
 }
 
@@ -311,7 +312,7 @@ int radix_sort_u32(Handle& h, Slot kin, Slot vin, Slot kalt, Slot valt, int64_t 
     return OGX_OK;
 }
 
-int radix_sort_key72(Handle& h, int64_t n, uint64_t** khi, uint32_t** klo, uint32_t** idx) {
+int radix_sort_key72(Handle& h, int64_t n, int first_pass, uint64_t** khi, uint32_t** klo, uint32_t** idx) {
     uint64_t *h0, *h1;
     uint32_t *l0, *l1, *i0, *i1;
     OGX_TRY(arena_get(h.ws, S_KHI, n, &h0));
@@ -321,7 +322,7 @@ int radix_sort_key72(Handle& h, int64_t n, uint64_t** khi, uint32_t** klo, uint3
     OGX_TRY(arena_get(h.ws, S_KLO2, n, &l1));
     OGX_TRY(arena_get(h.ws, S_IDX2, n, &i1));
     int which = 0;
-    if (n > 0) OGX_TRY(radix_passes(h, Key72{h0, l0}, Key72{h1, l1}, i0, i1, n, 9, &which));
+    if (n > 0) OGX_TRY(radix_passes(h, Key72{h0, l0}, Key72{h1, l1}, i0, i1, n, 9, &which, first_pass));
     *khi = which ? h1 : h0;
     *klo = which ? l1 : l0;
     *idx = which ? i1 : i0;

@@ -332,6 +332,15 @@ __global__ void k_nonleaf_offsets(const DevCounts* counts, int* nl_off) {
     nl_off[kMaxDepth + 1] = c;
 }
 
+// After a sort by levels 1..16 only (digit passes 3..8): flags a level-16 box that
+// holds more than thr bodies, i.e. bodies whose leaf may lie deeper, for which the
+// order of the lower digits matters.  Keys of one box are contiguous, so such a box
+// has two keys thr apart with the same 48-bit prefix (bits 15..62 of the high word).
+__global__ void k_deep_check(const uint64_t* __restrict__ khi, int64_t n, int thr, DevCounts* counts) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i + thr < n && (khi[i] >> 15) == (khi[i + thr] >> 15)) counts->deep_flag = 1;
+}
+
 inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
 static inline int bits_for(int64_t v) {
     int b = 1;
@@ -357,11 +366,11 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
 
     uint64_t* khi;
     uint32_t *klo, *kidx;
-    OGX_TRY(arena_get(h.ws, S_KHI, n, &khi));
-    OGX_TRY(arena_get(h.ws, S_KLO, n, &klo));
-    OGX_TRY(arena_get(h.ws, S_IDX, n, &kidx));
-    k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi, klo, kidx); ++h.launches;
-    OGX_TRY(radix_sort_key72(h, n, &khi, &klo, &kidx));
+    uint64_t* khi_in;
+    uint32_t *klo_in, *kidx_in;
+    OGX_TRY(arena_get(h.ws, S_KHI, n, &khi_in));
+    OGX_TRY(arena_get(h.ws, S_KLO, n, &klo_in));
+    OGX_TRY(arena_get(h.ws, S_IDX, n, &kidx_in));
 
     int *dfirst, *leaflev, *cnt, *leafflag, *leafstart, *level_off_dev;
     signed char* cplthr;
@@ -375,19 +384,31 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     leafscan = recoff + (n + 1);
     OGX_TRY(arena_get(h.ws, S_LEAFSTART, n + 2 + kMaxDepth + 2, &leafstart));
     level_off_dev = leafstart + n + 2;
-
-    k_topo_pairs<<<grid_for(n, 256), 256, 0, st>>>(khi, klo, n, thr, dfirst, cplthr); ++h.launches;
     const size_t wm_smem = WM_BLOCK + thr + 16;
     if (wm_smem > 48 * 1024) {
         OGX_CUDA(cudaFuncSetAttribute(k_topo_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wm_smem));
     }
-    k_topo_levels<<<grid_for(n, WM_BLOCK), WM_BLOCK, wm_smem, st>>>(cplthr, dfirst, n, thr, root, leaflev, cnt, leafflag, dc); ++h.launches;
-    OGX_TRY(scan_i32_to_i64(h, cnt, recoff, n));
-    OGX_TRY(scan_i32_to_i64(h, leafflag, leafscan, n));
-    k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev); ++h.launches;
-    // sync point 1: box / leaf / level counts
-    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaStreamSynchronize(st));
+
+    // Leaves need the key order only down to their own level.  First attempt: sort
+    // by levels 1..16 (6 of the 9 digit passes); if some level-16 box holds more than
+    // thr bodies (deep clusters) the counts read at sync point 1 say so and the build
+    // is repeated with the full 72-bit sort.
+    for (int attempt = 0;; ++attempt) {
+        const int first_pass = (attempt == 0) ? 3 : 0;
+        if (attempt > 0) OGX_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCounts), st));
+        k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi_in, klo_in, kidx_in); ++h.launches;
+        OGX_TRY(radix_sort_key72(h, n, first_pass, &khi, &klo, &kidx));
+        if (first_pass > 0 && n > thr) { k_deep_check<<<grid_for(n, 256), 256, 0, st>>>(khi, n, thr, dc); ++h.launches; }
+        k_topo_pairs<<<grid_for(n, 256), 256, 0, st>>>(khi, klo, n, thr, dfirst, cplthr); ++h.launches;
+        k_topo_levels<<<grid_for(n, WM_BLOCK), WM_BLOCK, wm_smem, st>>>(cplthr, dfirst, n, thr, root, leaflev, cnt, leafflag, dc); ++h.launches;
+        OGX_TRY(scan_i32_to_i64(h, cnt, recoff, n));
+        OGX_TRY(scan_i32_to_i64(h, leafflag, leafscan, n));
+        k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev); ++h.launches;
+        // sync point 1: box / leaf / level counts
+        OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+        OGX_CUDA(cudaStreamSynchronize(st));
+        if (!h.h_counts->deep_flag || first_pass == 0) break;
+    }
     const int nb = (int)h.h_counts->num_boxes;
     const int nleaf = (int)h.h_counts->num_leaves;
     h.max_level = h.h_counts->max_level;
