@@ -35,6 +35,8 @@ struct HarmTables {
     // gradient-coefficient constants (derivative recurrences of FmmExpansions3D.hpp:111-129)
     double gz[kTab][kTab], gp[kTab][kTab], gm[kTab][kTab];  // local  -> degree n (from degree n+1)
     double hz[kTab][kTab], hp[kTab][kTab], hm[kTab][kTab];  // mpole  -> degree n (from degree n-1)
+    // FP32 copies of the recurrence constants for the FP32 kernels (no conversion per use)
+    float fa[kTab], fb[kTab], fA[kTab][kTab], fB[kTab][kTab];
 };
 
 // the reference's derivative coefficients (FmmExpansions3D.hpp:111-129)
@@ -58,12 +60,18 @@ static inline void fill_harm_tables(HarmTables& t) {
         t.a[m] = m > 0 ? std::sqrt((2.0 * m - 1.0) / (2.0 * m)) : 1.0;
         t.b[m] = std::sqrt(2.0 * m + 1.0);
     }
+    for (int m = 0; m < kTab; ++m) {
+        t.fa[m] = (float)t.a[m];
+        t.fb[m] = (float)t.b[m];
+    }
     for (int n = 0; n < kTab; ++n)
         for (int m = 0; m < kTab; ++m) {
             if (n >= m + 2) {
                 const double d = std::sqrt((double)(n * n - m * m));
                 t.A[n][m] = (2.0 * n - 1.0) / d;
                 t.B[n][m] = std::sqrt((double)((n - 1) * (n - 1) - m * m)) / d;
+                t.fA[n][m] = (float)t.A[n][m];
+                t.fB[n][m] = (float)t.B[n][m];
             }
             if (m <= n) {
                 // G_n^m from L_{n+1}^{m}, L_{n+1}^{m-1}, L_{n+1}^{m+1}
@@ -101,6 +109,20 @@ static inline int harm_tables_ready(int device) {
 __host__ __device__ __forceinline__ constexpr int dof_re(int n, int m) { return m == 0 ? n * n : n * n + 2 * m - 1; }
 
 // Visit R_n^m(x,y,z), n <= P (m >= 0), calling f(n, m, re, im) column by column.
+// recurrence constants in the arithmetic type (FP32 kernels read the FP32 copies)
+template <class T> __device__ __forceinline__ T harm_a(int m) {
+    if constexpr (sizeof(T) == 4) return c_harm.fa[m]; else return (T)c_harm.a[m];
+}
+template <class T> __device__ __forceinline__ T harm_b(int m) {
+    if constexpr (sizeof(T) == 4) return c_harm.fb[m]; else return (T)c_harm.b[m];
+}
+template <class T> __device__ __forceinline__ T harm_A(int n, int m) {
+    if constexpr (sizeof(T) == 4) return c_harm.fA[n][m]; else return (T)c_harm.A[n][m];
+}
+template <class T> __device__ __forceinline__ T harm_B(int n, int m) {
+    if constexpr (sizeof(T) == 4) return c_harm.fB[n][m]; else return (T)c_harm.B[n][m];
+}
+
 template <int P, class T, class F>
 __device__ __forceinline__ void for_regular(T x, T y, T z, F&& f) {
     const T r2 = x * x + y * y + z * z;
@@ -108,20 +130,20 @@ __device__ __forceinline__ void for_regular(T x, T y, T z, F&& f) {
 #pragma unroll
     for (int m = 0; m <= P; ++m) {
         if (m > 0) {
-            const T a = (T)c_harm.a[m];
+            const T a = harm_a<T>(m);
             const T nr = a * (x * dr - y * di), ni = a * (x * di + y * dr);
             dr = nr;
             di = ni;
         }
         f(m, m, dr, di);
         if (m + 1 <= P) {
-            const T bz = (T)c_harm.b[m] * z;
+            const T bz = harm_b<T>(m) * z;
             T pr = dr, pi = di;              // R_{n-2}
             T cr = bz * dr, ci = bz * di;    // R_{n-1}
             f(m + 1, m, cr, ci);
 #pragma unroll
             for (int n = m + 2; n <= P; ++n) {
-                const T A = (T)c_harm.A[n][m] * z, B = (T)c_harm.B[n][m] * r2;
+                const T A = harm_A<T>(n, m) * z, B = harm_B<T>(n, m) * r2;
                 const T qr = A * cr - B * pr, qi = A * ci - B * pi;
                 pr = cr; pi = ci; cr = qr; ci = qi;
                 f(n, m, cr, ci);
@@ -136,24 +158,26 @@ template <int P, class T, class F>
 __device__ __forceinline__ void for_singular(T x, T y, T z, F&& f) {
     const T r2 = x * x + y * y + z * z;
     const T ir2 = T(1) / r2;
+    const T zr = z * ir2;      // FP32 path: one product per visit instead of two
     T dr = sqrt(ir2), di = 0;  // S_0^0 = 1/rho
 #pragma unroll
     for (int m = 0; m <= P; ++m) {
         if (m > 0) {
-            const T a = (T)c_harm.a[m] * ir2;
+            const T a = harm_a<T>(m) * ir2;
             const T nr = a * (x * dr - y * di), ni = a * (x * di + y * dr);
             dr = nr;
             di = ni;
         }
         f(m, m, dr, di);
         if (m + 1 <= P) {
-            const T bz = (T)c_harm.b[m] * z * ir2;
+            const T bz = (sizeof(T) == 4) ? harm_b<T>(m) * zr : harm_b<T>(m) * z * ir2;
             T pr = dr, pi = di;
             T cr = bz * dr, ci = bz * di;
             f(m + 1, m, cr, ci);
 #pragma unroll
             for (int n = m + 2; n <= P; ++n) {
-                const T A = (T)c_harm.A[n][m] * z * ir2, B = (T)c_harm.B[n][m] * ir2;
+                const T A = (sizeof(T) == 4) ? harm_A<T>(n, m) * zr : harm_A<T>(n, m) * z * ir2;
+                const T B = harm_B<T>(n, m) * ir2;
                 const T qr = A * cr - B * pr, qi = A * ci - B * pi;
                 pr = cr; pi = ci; cr = qr; ci = qi;
                 f(n, m, cr, ci);
