@@ -92,9 +92,9 @@ int ensure_operator_tables(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_OPS_M2L, ops->m2l.size(), &h.d_m2l));
     OGX_TRY(arena_get(h.ws, S_OPS_M2M, ops->m2m.size(), &h.d_m2m));
     OGX_TRY(arena_get(h.ws, S_OPS_L2L, ops->l2l.size(), &h.d_l2l));
-    OGX_CUDA(cudaMemcpy(h.d_m2l, ops->m2l.data(), ops->m2l.size() * sizeof(double), cudaMemcpyHostToDevice));
-    OGX_CUDA(cudaMemcpy(h.d_m2m, ops->m2m.data(), ops->m2m.size() * sizeof(double), cudaMemcpyHostToDevice));
-    OGX_CUDA(cudaMemcpy(h.d_l2l, ops->l2l.data(), ops->l2l.size() * sizeof(double), cudaMemcpyHostToDevice));
+    OGX_CUDA(upload_now(h.d_m2l, ops->m2l.data(), ops->m2l.size() * sizeof(double)));
+    OGX_CUDA(upload_now(h.d_m2m, ops->m2m.data(), ops->m2m.size() * sizeof(double)));
+    OGX_CUDA(upload_now(h.d_l2l, ops->l2l.data(), ops->l2l.size() * sizeof(double)));
     h.ops_p = h.prm.p;
     return OGX_OK;
 }

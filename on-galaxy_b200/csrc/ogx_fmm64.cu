@@ -381,9 +381,10 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
 // ---- mixed form ---------------------------------------------------------------------
 // host emulation of cvt.rna.tf32.f32 (round to nearest, ties away from zero)
 
-// Operator images for the tensor-core M2L, per offset o, K-chunk c and part (hi, lo):
-// rows = output dofs 1..K-1, K-major in the canonical no-swizzle core-matrix layout,
-// exactly the bytes one pipeline stage holds, so one bulk copy moves a chunk.
+// Operator images for the tensor-core M2L, per offset o, column slice z, K-chunk c
+// and part (hi, lo): rows = the slice's output dofs (all of 1..K-1 when there is one
+// slice), K-major in the 128-byte-swizzle layout, exactly the bytes one pipeline
+// stage holds, so one bulk copy moves a chunk.
 // Also row 0 of every T_o (for the degree-0 local coefficient of potentials).
 template <int P>
 int ensure_mixed_tables(Handle& h) {
@@ -391,7 +392,7 @@ int ensure_mixed_tables(Handle& h) {
     if (h.mix_ready_p == P) return OGX_OK;
     const int K = C::K;
     std::vector<double> T((size_t)K * K);
-    std::vector<uint8_t> img((size_t)343 * C::NCH * 2 * C::B_BYTES, 0);
+    std::vector<uint8_t> img((size_t)343 * C::NSPLIT * C::NCH * 2 * C::B_BYTES, 0);
     std::vector<double> row0((size_t)343 * K, 0.0);
     std::vector<float> ounscale(343, 0.f);
     for (int o = 0; o < 343; ++o) {
@@ -401,20 +402,22 @@ int ensure_mixed_tables(Handle& h) {
         for (int k = 0; k < K; ++k) row0[(size_t)o * K + k] = T[k];
         // FP16 images of T_o * 2^-e, largest used entry in [0.5, 1); 2^e undoes it
         double mx = 0.0;
-        for (int jr = 0; jr < C::N; ++jr)
+        for (int jr = 0; jr < C::NFULL; ++jr)
             for (int k = 0; k < K; ++k) mx = std::max(mx, std::fabs(T[(size_t)(jr + 1) * K + k]));
         int e = 0;
         if (mx > 0.0) std::frexp(mx, &e);
         const double scale = std::ldexp(1.0, -e);
         ounscale[o] = std::ldexp(1.0f, e);
+        // slice z, row jr holds output dof 1 + z N + jr
+        for (int z = 0; z < C::NSPLIT; ++z)
         for (int c = 0; c < C::NCH; ++c) {
-            uint8_t* hi = img.data() + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
+            uint8_t* hi = img.data() + ((size_t)((o * C::NSPLIT + z) * C::NCH + c) * 2) * C::B_BYTES;
             uint8_t* lo = hi + C::B_BYTES;
             for (int jr = 0; jr < C::N; ++jr)
                 for (int kk = 0; kk < C::CH * 16; ++kk) {
-                    const int k = c * C::CH * 16 + kk;
-                    if (k >= K) continue;
-                    const double x = T[(size_t)(jr + 1) * K + k] * scale;
+                    const int k = c * C::CH * 16 + kk, dof = 1 + z * C::N + jr;
+                    if (k >= K || dof >= K) continue;
+                    const double x = T[(size_t)dof * K + k] * scale;
                     const __half vh = __double2half(x);
                     const __half vl = __double2half(x - (double)__half2float(vh));
                     const int off = mixed::tile_off(jr, kk);
@@ -429,9 +432,9 @@ int ensure_mixed_tables(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_MIX_TOPS, img.size(), &d_img));
     OGX_TRY(arena_get(h.ws, S_MIX_ROW0, row0.size(), &d_row0));
     OGX_TRY(arena_get(h.ws, S_MIX_OUNSCALE, ounscale.size(), &d_ous));
-    OGX_CUDA(cudaMemcpy(d_img, img.data(), img.size(), cudaMemcpyHostToDevice));
-    OGX_CUDA(cudaMemcpy(d_row0, row0.data(), row0.size() * sizeof(double), cudaMemcpyHostToDevice));
-    OGX_CUDA(cudaMemcpy(d_ous, ounscale.data(), ounscale.size() * sizeof(float), cudaMemcpyHostToDevice));
+    OGX_CUDA(upload_now(d_img, img.data(), img.size()));
+    OGX_CUDA(upload_now(d_row0, row0.data(), row0.size() * sizeof(double)));
+    OGX_CUDA(upload_now(d_ous, ounscale.data(), ounscale.size() * sizeof(float)));
     h.d_tc_img = d_img;
     h.d_tc_row0 = d_row0;
     h.d_tc_ounscale = d_ous;
@@ -504,14 +507,14 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     if (h.ntgt > 0) {
         if constexpr (C::SUPPORTED) {
             OGX_CUDA(cudaFuncSetAttribute(mixed::k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-            mixed::k_m2l_tc<P><<<h.ntgt_pad / 128, C::THREADS, C::SMEM, st>>>(
+            mixed::k_m2l_tc<P><<<dim3(h.ntgt_pad / 128, C::NSPLIT), C::THREADS, C::SMEM, st>>>(
                 tv, h.tgt_tile_key, h.tgt_tile_box, mhi, mlo, mus, h.d_tc_img, h.d_tc_ounscale, Lown, h.d_err); ++h.launches;
             if (d_pot) {
                 mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, st>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,
                                                                              h.d_tc_row0, M, Lown); ++h.launches;
             }
         } else {
-            // p > 10: the accumulators of one tile do not fit TMEM; the FP64 M2L serves these orders
+            // an order whose operand would not fit TMEM even in slices: the FP64 M2L serves it
             const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
             OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
             k_m2l_fp64<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M,

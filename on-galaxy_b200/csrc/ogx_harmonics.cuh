@@ -98,6 +98,9 @@ static inline int harm_tables_ready(int device) {
     fill_harm_tables(t);
     cudaError_t e = cudaMemcpyToSymbol(c_harm, &t, sizeof(t));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_harm, &t, sizeof(t));
+    // the copies from the pageable t may still be in flight on the legacy stream,
+    // which the library's non-blocking streams do not wait for
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     if (e != cudaSuccess) {
         set_last_error(OGX_ERR_CUDA, std::string("harmonic tables: ") + cudaGetErrorString(e));
         return OGX_ERR_CUDA;

@@ -88,6 +88,17 @@ struct Arena {
     void release();
 };
 
+// Host-to-device copy of set-up data (operator tables) that has landed when this
+// returns.  cudaMemcpy from pageable host memory returns once the data is staged,
+// with the DMA still queued on the legacy stream, and the library's kernels run on
+// non-blocking streams that are not ordered after it; the synchronize closes that
+// window (it showed when several handles shared the copy engines).
+inline cudaError_t upload_now(void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+
 template <class T>
 inline int arena_get(Arena& a, Slot s, size_t count, T** out) {
     void* p = nullptr;

@@ -36,8 +36,11 @@
 // An MMA of N <= ~160 columns costs about the same time, so for p <= 8 the
 // operator's hi and lo images form one N = 2 N operand: A_hi x [B_hi | B_lo] and
 // A_lo x B_hi are two MMAs per K step (three otherwise).  TMEM holds two FP32
-// buffers (2 x 2N or 2 x N columns) + 2 x N FP64-halves columns, so the
-// tensor-core path serves p <= 10 (N <= 128); higher orders use the FP64 M2L kernel.
+// buffers (2 x 2N or 2 x N columns) + 2 x N FP64-halves columns, which fits
+// N <= 128 (p <= 10).  For p = 11 and 12 the output columns are cut into NSPLIT
+// slices (2 x 72 and 3 x 56 dofs), each handled by its own CTA (grid y) in the
+// paired form with one 64- or 80-column operand; the A rows are gathered once per
+// slice.
 //
 // Near field in FP32 on leaf-centred double-float coordinates (hi + lo FP32
 // relative to the target leaf centre, shift in FP64), r^-1 from rsqrt plus one
@@ -53,6 +56,16 @@
 namespace ogx {
 namespace mixed {
 
+// column slices of the M2L output: 1 while the unsplit operand fits TMEM (4 NPAD
+// <= 512), else the fewest slices whose width allows the paired form (6 NPAD <= 512)
+constexpr int tc_round16(int v) { return (v + 15) / 16 * 16; }
+constexpr int tc_nsplit(int nfull) {
+    if (4 * tc_round16(nfull) <= 512) return 1;
+    int s = 2;
+    while (6 * tc_round16((nfull + s - 1) / s) > 512) ++s;
+    return s;
+}
+
 template <int P>
 struct TcCfg {
     static constexpr int K = (P + 1) * (P + 1);
@@ -60,7 +73,9 @@ struct TcCfg {
     static constexpr int NKS = KPAD / 16;     // K-steps of the MMA (16 fp16 each)
     static constexpr int CH = 4;              // K-steps per pipeline chunk (64 fp16 = one 128-byte line)
     static constexpr int NCH = (NKS + CH - 1) / CH;
-    static constexpr int N = K - 1;           // output dofs 1..K-1
+    static constexpr int NFULL = K - 1;       // output dofs 1..K-1
+    static constexpr int NSPLIT = tc_nsplit(NFULL);
+    static constexpr int N = (NFULL + NSPLIT - 1) / NSPLIT;   // dofs of one slice: 1 + z N .. z N + N
     static constexpr int NPAD = (N + 15) / 16 * 16;
     static constexpr int M = 128;
     static constexpr int SBO = 1024;          // bytes between 8-row groups (one swizzle atom)
@@ -153,7 +168,8 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
              const __half* __restrict__ mhi, const __half* __restrict__ mlo, const float* __restrict__ munscale,
              const uint8_t* __restrict__ btab, const float* __restrict__ ounscale, double* __restrict__ lown, int* err) {
     using C = TcCfg<P>;
-    static_assert(C::SUPPORTED, "tensor-core M2L serves p <= 10");
+    static_assert(C::SUPPORTED, "tensor-core M2L: operand does not fit");
+    const int zs = blockIdx.y;                    // output column slice
     // gathers kept in flight per producer thread before its row is handed to the MMA
     constexpr int LAG = C::STAGES >= 4 ? C::STAGES - 2 : 1;
     constexpr int NG = C::NPAD / 16;
@@ -345,7 +361,7 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                 }
                 uint8_t* st = smem + (size_t)s * C::STAGE_BYTES;
                 if (r == 0) {
-                    const uint8_t* bsrc = btab + ((size_t)(o * C::NCH + c) * 2) * C::B_BYTES;
+                    const uint8_t* bsrc = btab + ((size_t)((o * C::NSPLIT + zs) * C::NCH + c) * 2) * C::B_BYTES;
                     sm100::mbar_arrive_expect_tx(&bfull[s], 2 * C::B_BYTES);
                     sm100::bulk_g2s(st + 2 * C::A_BYTES, bsrc, C::B_BYTES, &bfull[s]);
                     sm100::bulk_g2s(st + 2 * C::A_BYTES + C::B_BYTES, bsrc + C::B_BYTES, C::B_BYTES, &bfull[s]);
@@ -444,8 +460,8 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                         if (c16 < g1) {
 #pragma unroll
                             for (int i = 0; i < 16; ++i) {
-                                const int dof = 1 + c16 * 16 + i;
-                                if (dof < C::K) lown[(size_t)myb * C::K + dof] += racc[g][i] * inv;
+                                const int col = c16 * 16 + i, dof = 1 + zs * C::N + col;
+                                if (col < C::N && dof < C::K) lown[(size_t)myb * C::K + dof] += racc[g][i] * inv;
                             }
                         }
                     }
@@ -461,8 +477,8 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                     if (myb >= 0) {
 #pragma unroll
                         for (int k = 0; k < 16; ++k) {
-                            const int dof = 1 + c16 * 16 + k;
-                            if (dof < C::K)
+                            const int col = c16 * 16 + k, dof = 1 + zs * C::N + col;
+                            if (col < C::N && dof < C::K)
                                 lown[(size_t)myb * C::K + dof] += __hiloint2double((int)hi[k], (int)lo[k]) * inv;
                         }
                     }
