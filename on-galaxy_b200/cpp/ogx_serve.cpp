@@ -1,0 +1,333 @@
+// ogx_serve.cpp -- a serving loop for integration jobs on one GPU, through the C ABI.
+//
+// Jobs (a seeded stream): Poisson arrivals at --rate jobs/s, N log-uniform in
+// [--nmin, --nmax], p drawn from --orders, --smin..--smax leapfrog steps with dt 0.01,
+// half Plummer spheres, half two-galaxy disk+bulge systems.  A job is admitted when it
+// has arrived and its estimated device footprint fits the --hbm-gb budget next to the
+// jobs already running; it then runs on its own handle (own streams) and host thread,
+// with bodies, tree and expansions resident on the device until it finishes, so jobs
+// that arrive while others run overlap with them on the GPU and free their memory
+// when done (continuous admission, not a queue drained one job at a time).
+// --solo runs the same jobs one after another with nothing else on the GPU.
+//
+// Prints one JSON line: per-step latency p50 / p99 (the time from a step call until its
+// result is on the device, ogx_step + ogx_synchronize, as a client waiting on it sees it),
+// aggregate bodies*steps/s over the wall time, the peak number of concurrent jobs, and
+// per job an FNV-1a digest of its final positions and velocities (bit-exact), which the
+// tests compare between --solo and the mixed run.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ogx.h"
+
+namespace {
+
+struct Job {
+    int id = 0;
+    double arrival = 0.0;  // seconds after start
+    int64_t n = 0;
+    int p = 8;
+    int steps = 10;
+    int kind = 0;  // 0 Plummer, 1 two-galaxy disk+bulge
+    uint64_t seed = 0;
+    // results
+    uint64_t digest = 0;
+    std::vector<float> step_ms;
+    int status = OGX_OK;
+    bool rejected = false;   // footprint above the whole budget: never admitted
+    double need_bytes = 0.0;  // admission estimate
+    double peak_bytes = 0.0;  // device memory above the idle level while it ran (--solo only)
+};
+
+// Plummer sphere (a = 1, M = 1, G = 1) drawn on the host: enclosed-mass inverse for
+// r (cut at 20 a), isotropic directions, speed fraction by rejection from
+// q^2 (1 - q^2)^(7/2), centre of mass and momentum removed
+void plummer(int64_t n, uint64_t seed, std::vector<double>& pos, std::vector<double>& vel, std::vector<double>& mass) {
+    std::mt19937_64 rng(seed);
+    auto uni = [&]() { return (double)(rng() >> 11) * (1.0 / 9007199254740992.0); };
+    pos.assign(3 * n, 0.0);
+    vel.assign(3 * n, 0.0);
+    mass.assign(n, 1.0 / (double)n);
+    const double umax = std::pow(20.0, 3) / std::pow(20.0 * 20.0 + 1.0, 1.5);
+    double cp[3] = {0, 0, 0}, cv[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i) {
+        const double u = std::max(uni() * umax, 1e-12);
+        const double r = 1.0 / std::sqrt(std::pow(u, -2.0 / 3.0) - 1.0);
+        double q, g;
+        do {
+            q = uni();
+            g = 0.1 * uni();
+        } while (g > q * q * std::pow(1.0 - q * q, 3.5));
+        const double v = q * std::sqrt(2.0) * std::pow(r * r + 1.0, -0.25);
+        for (int pass = 0; pass < 2; ++pass) {
+            const double cz = 2.0 * uni() - 1.0, sz = std::sqrt(std::max(0.0, 1.0 - cz * cz)), ph = 2.0 * M_PI * uni();
+            const double len = pass == 0 ? r : v;
+            double* o = (pass == 0 ? pos.data() : vel.data()) + 3 * i;
+            o[0] = len * sz * std::cos(ph);
+            o[1] = len * sz * std::sin(ph);
+            o[2] = len * cz;
+        }
+        for (int k = 0; k < 3; ++k) {
+            cp[k] += pos[3 * i + k] / (double)n;
+            cv[k] += vel[3 * i + k] / (double)n;
+        }
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            pos[3 * i + k] -= cp[k];
+            vel[3 * i + k] -= cv[k];
+        }
+}
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull) {
+    const unsigned char* c = (const unsigned char*)data;
+    for (size_t i = 0; i < bytes; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+// admission estimate of a job's device footprint: the per-order operator tables
+// (343 M2L matrices of K^2 doubles, with room for the mixed form's images) and per
+// body its coordinates, keys, tree, lists and expansions; measured peaks sit below
+// it by 20-50% from 16k to 200k bodies at p = 6, 8 and 12
+double footprint_bytes(int64_t n, int p) {
+    const double K = (double)(p + 1) * (p + 1);
+    return 48e6 + 343.0 * K * K * 8.0 * 1.5 + (double)n * (1300.0 + 1.5 * K);
+}
+
+void run_job(Job& job, int precision) {
+    ogx_params prm;
+    ogx_params_default(&prm);
+    prm.p = job.p;
+    prm.leaf_capacity = 64;
+    prm.precision = precision;
+    void* h = nullptr;
+    if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return;
+    if (job.kind == 0) {
+        std::vector<double> pos, vel, mass;
+        plummer(job.n, job.seed, pos, vel, mass);
+        job.status = ogx_upload(h, job.n, pos.data(), vel.data(), mass.data());
+    } else {
+        ogx_merger_params mp;
+        ogx_merger_params_default(&mp);
+        mp.n_per = job.n / 2;
+        mp.seed = job.seed;
+        job.status = ogx_ic_merger(h, &mp, nullptr);
+    }
+    if (job.status != OGX_OK) {
+        ogx_destroy(h);
+        return;
+    }
+    const int64_t n = (job.kind == 0) ? job.n : 2 * (job.n / 2);
+    for (int s = 0; s < job.steps && job.status == OGX_OK; ++s) {
+        const auto t0 = std::chrono::steady_clock::now();
+        job.status = ogx_step(h, 0.01, 1);
+        if (job.status == OGX_OK) job.status = ogx_synchronize(h);
+        job.step_ms.push_back(
+            (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+    std::vector<double> pos(3 * n), vel(3 * n);
+    if (job.status == OGX_OK) job.status = ogx_download(h, pos.data(), vel.data(), nullptr);
+    job.digest = fnv1a(vel.data(), vel.size() * 8, fnv1a(pos.data(), pos.size() * 8));
+    ogx_destroy(h);
+}
+
+// samples the device's used memory every millisecond while armed (solo runs)
+struct MemSampler {
+    std::atomic<bool> stop{false}, armed{false};
+    std::atomic<double> peak{0.0};
+    std::thread th;
+    void start() {
+        th = std::thread([this]() {
+            cudaSetDevice(0);
+            while (!stop.load()) {
+                size_t fr = 0, tot = 0;
+                if (armed.load() && cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+                    const double used = (double)(tot - fr);
+                    double cur = peak.load();
+                    while (used > cur && !peak.compare_exchange_weak(cur, used)) {
+                    }
+                }
+                std::this_thread::sleep_for(std::chrono::milliseconds(1));
+            }
+        });
+    }
+    void finish() {
+        stop = true;
+        if (th.joinable()) th.join();
+    }
+};
+
+double device_used() {
+    size_t fr = 0, tot = 0;
+    return cudaMemGetInfo(&fr, &tot) == cudaSuccess ? (double)(tot - fr) : 0.0;
+}
+
+double percentile(std::vector<float> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * (double)(v.size() - 1);
+    const size_t lo = (size_t)pos;
+    const size_t hi = std::min(lo + 1, v.size() - 1);
+    return v[lo] + (pos - (double)lo) * (v[hi] - v[lo]);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    int njobs = 24, smin = 10, smax = 200;
+    double rate = 20.0, hbm_gb = 150.0;
+    int64_t nmin = 16384, nmax = 1 << 20;
+    uint64_t seed = 1;
+    bool solo = false;
+    int precision = OGX_PREC_MIXED;
+    std::vector<int> orders = {6, 8, 12};
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto next = [&]() -> std::string { return (i + 1 < argc) ? argv[++i] : ""; };
+        if (a == "--jobs") njobs = std::atoi(next().c_str());
+        else if (a == "--rate") rate = std::atof(next().c_str());
+        else if (a == "--nmin") nmin = std::atoll(next().c_str());
+        else if (a == "--nmax") nmax = std::atoll(next().c_str());
+        else if (a == "--smin") smin = std::atoi(next().c_str());
+        else if (a == "--smax") smax = std::atoi(next().c_str());
+        else if (a == "--hbm-gb") hbm_gb = std::atof(next().c_str());
+        else if (a == "--seed") seed = std::strtoull(next().c_str(), nullptr, 10);
+        else if (a == "--solo") solo = true;
+        else if (a == "--precision") precision = (next() == "fp64") ? OGX_PREC_FP64 : OGX_PREC_MIXED;
+        else if (a == "--orders") {
+            orders.clear();
+            std::string v = next();
+            for (size_t s = 0; s < v.size();) {
+                const size_t e = v.find(',', s);
+                orders.push_back(std::atoi(v.substr(s, e == std::string::npos ? std::string::npos : e - s).c_str()));
+                if (e == std::string::npos) break;
+                s = e + 1;
+            }
+        } else {
+            std::fprintf(stderr, "unknown option %s\n", a.c_str());
+            return 2;
+        }
+    }
+    if (njobs < 1 || nmin < 2 || nmax < nmin || smin < 1 || smax < smin || orders.empty() || rate <= 0) {
+        std::fprintf(stderr, "bad arguments\n");
+        return 2;
+    }
+    // the seeded job stream
+    std::mt19937_64 rng(seed);
+    auto uni = [&]() { return (double)(rng() >> 11) * (1.0 / 9007199254740992.0); };
+    std::vector<Job> jobs(njobs);
+    double t = 0.0;
+    for (int j = 0; j < njobs; ++j) {
+        t += -std::log(1.0 - uni()) / rate;
+        Job& jb = jobs[j];
+        jb.id = j;
+        jb.arrival = t;
+        jb.n = (int64_t)std::llround(std::exp(std::log((double)nmin) + uni() * (std::log((double)nmax) - std::log((double)nmin))));
+        jb.p = orders[(size_t)(uni() * orders.size()) % orders.size()];
+        jb.steps = smin + (int)(uni() * (smax - smin + 1)) % (smax - smin + 1);
+        jb.kind = j & 1;
+        jb.seed = seed * 1000003ull + (uint64_t)j;
+    }
+    {
+        // a device must be there before any job is admitted
+        ogx_params prm;
+        ogx_params_default(&prm);
+        void* probe = nullptr;
+        const int rc = ogx_create(&prm, &probe);
+        if (rc != OGX_OK) {
+            std::printf("{\"error\": \"%s\"}\n", ogx_strerror(rc));
+            return 3;
+        }
+        ogx_destroy(probe);
+    }
+    const double budget = hbm_gb * 1e9;
+    const auto start = std::chrono::steady_clock::now();
+    auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count(); };
+    std::mutex mu;
+    std::condition_variable cv;
+    double in_use = 0.0;
+    int running = 0, peak = 0;
+    std::vector<std::thread> threads;
+    MemSampler sampler;
+    if (solo) sampler.start();
+    const double idle = device_used();
+    int rejected = 0;
+    for (Job& jb : jobs) {
+        jb.need_bytes = footprint_bytes(jb.n, jb.p);
+        if (jb.need_bytes > budget) {
+            // could never fit, even alone: refused at admission, the loop goes on
+            jb.rejected = true;
+            jb.status = OGX_ERR_INVALID;
+            ++rejected;
+            continue;
+        }
+        if (solo) {
+            sampler.peak = 0.0;
+            sampler.armed = true;
+            run_job(jb, precision);
+            sampler.armed = false;
+            jb.peak_bytes = std::max(0.0, sampler.peak.load() - idle);
+            continue;
+        }
+        // wait for the arrival time, then for room under the budget
+        const double wait = jb.arrival - now_s();
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&]() { return running == 0 || in_use + jb.need_bytes <= budget; });
+        in_use += jb.need_bytes;
+        peak = std::max(peak, ++running);
+        lk.unlock();
+        threads.emplace_back([&, jp = &jb]() {
+            run_job(*jp, precision);
+            std::lock_guard<std::mutex> g(mu);
+            in_use -= jp->need_bytes;
+            --running;
+            cv.notify_all();
+        });
+    }
+    for (auto& th : threads) th.join();
+    sampler.finish();
+    const double wall = now_s();
+    std::vector<float> all;
+    double bodysteps = 0.0;
+    int failed = 0;
+    for (const Job& jb : jobs) {
+        all.insert(all.end(), jb.step_ms.begin(), jb.step_ms.end());
+        bodysteps += (double)jb.n * (double)jb.step_ms.size();
+        if (jb.status != OGX_OK && !jb.rejected) ++failed;
+    }
+    std::printf("{\"mode\": \"%s\", \"precision\": \"%s\", \"jobs\": %d, \"failed\": %d, \"rejected\": %d, "
+                "\"steps\": %zu, \"wall_s\": %.3f, \"bodies_steps_per_s\": %.6e, \"p50_step_ms\": %.3f, "
+                "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"jobs_detail\": [",
+                solo ? "solo" : "served", precision == OGX_PREC_FP64 ? "fp64" : "mixed", njobs, failed, rejected,
+                all.size(), wall, bodysteps / wall, percentile(all, 0.5), percentile(all, 0.99), solo ? 1 : peak,
+                hbm_gb);
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const Job& jb = jobs[j];
+        std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"steps\": %d, \"kind\": \"%s\", \"status\": %d, "
+                    "\"rejected\": %s, \"need_mb\": %.1f, \"peak_mb\": %.1f, \"step_ms_p50\": %.3f, "
+                    "\"digest\": \"%016llx\"}",
+                    j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.steps, jb.kind ? "disk+bulge merger" : "plummer",
+                    jb.status, jb.rejected ? "true" : "false", jb.need_bytes / 1e6, jb.peak_bytes / 1e6,
+                    percentile(jb.step_ms, 0.5), (unsigned long long)jb.digest);
+    }
+    std::printf("]}\n");
+    return failed ? 1 : 0;
+}

@@ -1,0 +1,96 @@
+"""The serving loop (on-galaxy_b200/cpp/ogx_serve.cpp): integration jobs from a seeded
+Poisson stream, admitted under a device-memory budget, each running with its state resident
+on the device while others run beside it.
+
+The reference has no serving loop; what carries over is its integrator
+(src3d/Integrator3D.hpp:23-40, one force evaluation per leapfrog step) and its initial
+conditions (Plummer, src3d/InitialConditions3D.hpp; disk+bulge mergers,
+src3d/gpu/GalaxyIC.hpp:43-125).  The property checked here is that a job's result does
+not depend on what else runs: the final positions and velocities of every job are
+bit-identical when it runs alone and when it shares the GPU.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SERVE = os.path.join(ROOT, "on-galaxy_b200", "ogx_serve")
+
+
+def _serve(*args, expect_rc=0):
+    if not os.path.exists(SERVE):
+        pytest.skip("ogx_serve not built")
+    r = subprocess.run([SERVE, *map(str, args)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == expect_rc, r.stdout[-2000:] + r.stderr[-2000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+SMALL = ("--jobs", 8, "--rate", 400, "--nmin", 16384, "--nmax", 200000, "--smin", 3, "--smax", 8,
+         "--orders", "6,8,12", "--seed", 7)
+
+
+def test_serve_rejects_bad_arguments():
+    if not os.path.exists(SERVE):
+        pytest.skip("ogx_serve not built")
+    r = subprocess.run([SERVE, "--jobs", "0"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+    r = subprocess.run([SERVE, "--nmin", "100", "--nmax", "10"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+
+
+def test_serve_reports_missing_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    out = _serve("--jobs", 2, expect_rc=3)
+    assert "error" in out
+
+
+@pytest.mark.gpu
+def test_jobs_give_the_same_bits_alone_and_in_the_mix():
+    solo = _serve(*SMALL, "--solo")
+    mixed = _serve(*SMALL)
+    assert solo["failed"] == 0 and mixed["failed"] == 0
+    assert solo["rejected"] == 0 and mixed["rejected"] == 0
+    # jobs overlapped on the GPU
+    assert mixed["peak_concurrent"] >= 2
+    a = {j["id"]: j for j in solo["jobs_detail"]}
+    b = {j["id"]: j for j in mixed["jobs_detail"]}
+    assert a.keys() == b.keys()
+    kinds = set()
+    for k in a:
+        assert (a[k]["n"], a[k]["p"], a[k]["steps"]) == (b[k]["n"], b[k]["p"], b[k]["steps"])
+        assert a[k]["digest"] == b[k]["digest"], f"job {k} differs when run in the mix"
+        kinds.add(a[k]["kind"])
+    assert len(kinds) == 2
+    assert solo["steps"] == mixed["steps"] == sum(j["steps"] for j in solo["jobs_detail"])
+    assert 0 < mixed["p50_step_ms"] <= mixed["p99_step_ms"]
+    # the admission estimate covers what each job used alone
+    for j in solo["jobs_detail"]:
+        assert j["peak_mb"] <= j["need_mb"], j
+
+
+@pytest.mark.gpu
+def test_jobs_above_the_budget_are_refused_and_the_rest_run():
+    out = _serve("--jobs", 6, "--rate", 400, "--nmin", 16384, "--nmax", 1 << 20, "--smin", 2, "--smax", 3,
+                 "--orders", "8", "--seed", 3, "--hbm-gb", 0.4)
+    assert out["failed"] == 0
+    refused = [j for j in out["jobs_detail"] if j["rejected"]]
+    ran = [j for j in out["jobs_detail"] if not j["rejected"]]
+    assert out["rejected"] == len(refused) >= 1 and len(ran) >= 1
+    assert all(j["need_mb"] > 400 for j in refused)
+    assert all(j["need_mb"] <= 400 and j["status"] == 0 for j in ran)
+    assert out["steps"] == sum(j["steps"] for j in ran)
+
+
+@pytest.mark.gpu
+def test_fp64_jobs_give_the_same_bits_alone_and_in_the_mix():
+    args = ("--jobs", 4, "--rate", 400, "--nmin", 16384, "--nmax", 65536, "--smin", 2, "--smax", 4,
+            "--orders", "6,8", "--seed", 11, "--precision", "fp64")
+    solo = _serve(*args, "--solo")
+    mixed = _serve(*args)
+    assert solo["precision"] == mixed["precision"] == "fp64"
+    assert [j["digest"] for j in solo["jobs_detail"]] == [j["digest"] for j in mixed["jobs_detail"]]
