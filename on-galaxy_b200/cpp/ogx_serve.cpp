@@ -4,17 +4,27 @@
 // [--nmin, --nmax], p drawn from --orders, --smin..--smax leapfrog steps with dt 0.01,
 // half Plummer spheres, half two-galaxy disk+bulge systems.  A job is admitted when it
 // has arrived and its estimated device footprint fits the --hbm-gb budget next to the
-// jobs already running; it then runs on its own handle (own streams) and host thread,
-// with bodies, tree and expansions resident on the device until it finishes, so jobs
-// that arrive while others run overlap with them on the GPU and free their memory
-// when done (continuous admission, not a queue drained one job at a time).
+// jobs already resident; it then keeps its own handle (own streams) with bodies, tree
+// and expansions on the device until it finishes and frees its memory.  A pool of
+// --workers host threads (default 8) runs the resident jobs' steps from one FIFO
+// queue, a job re-queued after each of its steps, so every resident job advances
+// while at most W steps are in flight on the GPU (continuous batching at step
+// granularity, not a queue drained one job at a time).  Before the clock starts, one
+// small job per order and initial-condition kind warms the server up.
 // --solo runs the same jobs one after another with nothing else on the GPU.
 //
+// --ensemble --steps S: the batched-ensemble workload instead.  All systems are
+// resident together and advance in lockstep (every system finishes step s before any
+// starts step s + 1), their steps spread over the same worker pool; the line then also
+// carries the lockstep step time (p50 / p99).  --autotune picks each system's leaf
+// capacity from {32, 48, 64, 96, 128} by timing force evaluations of that system alone
+// before the run; --thr fixes it instead (default 64).
+//
 // Prints one JSON line: per-step latency p50 / p99 (the time from a step call until its
-// result is on the device, ogx_step + ogx_synchronize, as a client waiting on it sees it),
-// aggregate bodies*steps/s over the wall time, the peak number of concurrent jobs, and
-// per job an FNV-1a digest of its final positions and velocities (bit-exact), which the
-// tests compare between --solo and the mixed run.
+// result is on the device, ogx_step + ogx_synchronize), job turnaround p50 / p99 (from
+// arrival to the final state on the host), aggregate bodies*steps/s over the wall time,
+// the peak number of resident jobs, and per job an FNV-1a digest of its final positions
+// and velocities (bit-exact), which the tests compare between --solo and the other modes.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -24,6 +34,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <random>
 #include <string>
@@ -43,6 +54,7 @@ struct Job {
     int p = 8;
     int steps = 10;
     int kind = 0;  // 0 Plummer, 1 two-galaxy disk+bulge
+    int thr = 64;  // leaf capacity
     uint64_t seed = 0;
     // results
     uint64_t digest = 0;
@@ -51,6 +63,8 @@ struct Job {
     bool rejected = false;   // footprint above the whole budget: never admitted
     double need_bytes = 0.0;  // admission estimate
     double peak_bytes = 0.0;  // device memory above the idle level while it ran (--solo only)
+    double t_done = 0.0;      // seconds after start when it finished
+    void* h = nullptr;        // its handle while resident
 };
 
 // Plummer sphere (a = 1, M = 1, G = 1) drawn on the host: enclosed-mass inverse for
@@ -103,22 +117,24 @@ uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603u
 }
 
 // admission estimate of a job's device footprint: the per-order operator tables
-// (343 M2L matrices of K^2 doubles, with room for the mixed form's images) and per
-// body its coordinates, keys, tree, lists and expansions; measured peaks sit below
-// it by 20-50% from 16k to 200k bodies at p = 6, 8 and 12
+// (343 M2L matrices of K^2 doubles and the mixed form's padded FP16 hi/lo images,
+// 20 bytes per matrix entry together, with slack) and per body its coordinates,
+// keys, tree, lists and expansions; measured peaks sit below it by 20-50% from
+// 16k to 200k bodies at p = 6, 8 and 12
 double footprint_bytes(int64_t n, int p) {
     const double K = (double)(p + 1) * (p + 1);
-    return 48e6 + 343.0 * K * K * 8.0 * 1.5 + (double)n * (1300.0 + 1.5 * K);
+    return 48e6 + 343.0 * K * K * 20.0 + (double)n * (1300.0 + 1.5 * K);
 }
 
-void run_job(Job& job, int precision) {
+// create the job's handle and its initial conditions on the device
+void* open_job(Job& job, int precision) {
     ogx_params prm;
     ogx_params_default(&prm);
     prm.p = job.p;
-    prm.leaf_capacity = 64;
+    prm.leaf_capacity = job.thr;
     prm.precision = precision;
     void* h = nullptr;
-    if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return;
+    if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return nullptr;
     if (job.kind == 0) {
         std::vector<double> pos, vel, mass;
         plummer(job.n, job.seed, pos, vel, mass);
@@ -132,20 +148,60 @@ void run_job(Job& job, int precision) {
     }
     if (job.status != OGX_OK) {
         ogx_destroy(h);
-        return;
+        return nullptr;
     }
+    return h;
+}
+
+// one leapfrog step, timed from the call until its result is on the device
+void step_job(Job& job, void* h) {
+    const auto t0 = std::chrono::steady_clock::now();
+    job.status = ogx_step(h, 0.01, 1);
+    if (job.status == OGX_OK) job.status = ogx_synchronize(h);
+    job.step_ms.push_back((float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+}
+
+// digest of the final positions and velocities, then release the handle
+void close_job(Job& job, void* h) {
     const int64_t n = (job.kind == 0) ? job.n : 2 * (job.n / 2);
-    for (int s = 0; s < job.steps && job.status == OGX_OK; ++s) {
-        const auto t0 = std::chrono::steady_clock::now();
-        job.status = ogx_step(h, 0.01, 1);
-        if (job.status == OGX_OK) job.status = ogx_synchronize(h);
-        job.step_ms.push_back(
-            (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-    }
     std::vector<double> pos(3 * n), vel(3 * n);
     if (job.status == OGX_OK) job.status = ogx_download(h, pos.data(), vel.data(), nullptr);
     job.digest = fnv1a(vel.data(), vel.size() * 8, fnv1a(pos.data(), pos.size() * 8));
     ogx_destroy(h);
+}
+
+void run_job(Job& job, int precision) {
+    void* h = open_job(job, precision);
+    if (!h) return;
+    for (int s = 0; s < job.steps && job.status == OGX_OK; ++s) step_job(job, h);
+    close_job(job, h);
+}
+
+// leaf capacity of a job from a short trial: the candidate whose second force
+// evaluation (a step of dt = 0 leaves the state unchanged) is fastest when run alone
+int autotune_thr(Job job, int precision) {
+    static const int cands[] = {32, 48, 64, 96, 128};
+    int best = job.thr;
+    float best_ms = 1e30f;
+    for (int thr : cands) {
+        job.thr = thr;
+        job.step_ms.clear();
+        void* h = open_job(job, precision);
+        if (!h) continue;
+        float ms = 1e30f;
+        for (int r = 0; r < 3 && job.status == OGX_OK; ++r) {
+            const auto t0 = std::chrono::steady_clock::now();
+            job.status = ogx_step(h, 0.0, 1);
+            if (job.status == OGX_OK) job.status = ogx_synchronize(h);
+            if (r > 0) ms = std::min(ms, (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+        }
+        ogx_destroy(h);
+        if (job.status == OGX_OK && ms < best_ms) {
+            best_ms = ms;
+            best = thr;
+        }
+    }
+    return best;
 }
 
 // samples the device's used memory every millisecond while armed (solo runs)
@@ -195,8 +251,8 @@ int main(int argc, char** argv) {
     double rate = 20.0, hbm_gb = 150.0;
     int64_t nmin = 16384, nmax = 1 << 20;
     uint64_t seed = 1;
-    bool solo = false;
-    int precision = OGX_PREC_MIXED;
+    bool solo = false, ensemble = false, autotune = false;
+    int precision = OGX_PREC_MIXED, thr = 64, workers = 8;
     std::vector<int> orders = {6, 8, 12};
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -210,6 +266,11 @@ int main(int argc, char** argv) {
         else if (a == "--hbm-gb") hbm_gb = std::atof(next().c_str());
         else if (a == "--seed") seed = std::strtoull(next().c_str(), nullptr, 10);
         else if (a == "--solo") solo = true;
+        else if (a == "--ensemble") ensemble = true;
+        else if (a == "--autotune") autotune = true;
+        else if (a == "--thr") thr = std::atoi(next().c_str());
+        else if (a == "--workers") workers = std::atoi(next().c_str());
+        else if (a == "--steps") smin = smax = std::atoi(next().c_str());
         else if (a == "--precision") precision = (next() == "fp64") ? OGX_PREC_FP64 : OGX_PREC_MIXED;
         else if (a == "--orders") {
             orders.clear();
@@ -225,7 +286,8 @@ int main(int argc, char** argv) {
             return 2;
         }
     }
-    if (njobs < 1 || nmin < 2 || nmax < nmin || smin < 1 || smax < smin || orders.empty() || rate <= 0) {
+    if (njobs < 1 || nmin < 2 || nmax < nmin || smin < 1 || smax < smin || orders.empty() || rate <= 0 || thr < 1 || workers < 1 ||
+        (ensemble && smin != smax)) {
         std::fprintf(stderr, "bad arguments\n");
         return 2;
     }
@@ -244,6 +306,8 @@ int main(int argc, char** argv) {
         jb.steps = smin + (int)(uni() * (smax - smin + 1)) % (smax - smin + 1);
         jb.kind = j & 1;
         jb.seed = seed * 1000003ull + (uint64_t)j;
+        jb.thr = thr;
+        if (ensemble) jb.arrival = 0.0;   // the whole ensemble starts together
     }
     {
         // a device must be there before any job is admitted
@@ -257,18 +321,188 @@ int main(int argc, char** argv) {
         }
         ogx_destroy(probe);
     }
+    // server start-up, before the clock: one small job per order and initial-condition
+    // kind loads every kernel module and builds the per-order operator tables, which
+    // a running server has done long before its jobs arrive
+    const auto w0 = std::chrono::steady_clock::now();
+    for (int p : orders)
+        for (int kind = 0; kind < 2; ++kind) {
+            Job w;
+            w.n = 4096;
+            w.p = p;
+            w.steps = 2;
+            w.kind = kind;
+            w.thr = thr;
+            w.seed = 12345;
+            run_job(w, precision);
+            if (w.status != OGX_OK) {
+                std::printf("{\"error\": \"warm-up job failed: %s\"}\n", ogx_strerror(w.status));
+                return 3;
+            }
+        }
+    const double warmup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
     const double budget = hbm_gb * 1e9;
-    const auto start = std::chrono::steady_clock::now();
-    auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count(); };
-    std::mutex mu;
-    std::condition_variable cv;
-    double in_use = 0.0;
-    int running = 0, peak = 0;
-    std::vector<std::thread> threads;
     MemSampler sampler;
     if (solo) sampler.start();
     const double idle = device_used();
-    int rejected = 0;
+    const auto start = std::chrono::steady_clock::now();
+    auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count(); };
+
+    // ---- the worker pool (served and ensemble modes) ----
+    // W host threads run the jobs' tasks: open (handle + initial conditions), step,
+    // close.  A job's next task is queued only when its previous one has finished,
+    // so no handle is used by two threads at once; the FIFO queue interleaves the
+    // steps of all resident jobs (continuous batching at step granularity) and W
+    // bounds the steps in flight on the GPU.
+    enum TaskKind { T_OPEN, T_STEP, T_CLOSE };
+    struct Task {
+        Job* job;
+        TaskKind kind;
+    };
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Task> queue;
+    bool quit = false, lockstep = false;
+    int finished = 0, step_done = 0, running = 0, peak = 0, rejected = 0;
+    double in_use = 0.0;
+    auto push = [&](Job* j, TaskKind k) {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            queue.push_back({j, k});
+        }
+        cv_work.notify_one();
+    };
+    auto worker = [&]() {
+        for (;;) {
+            Task t;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&]() { return quit || !queue.empty(); });
+                if (queue.empty()) return;
+                t = queue.front();
+                queue.pop_front();
+            }
+            Job& jb = *t.job;
+            if (t.kind == T_OPEN) {
+                jb.h = open_job(jb, precision);
+                if (lockstep) {
+                    std::lock_guard<std::mutex> g(mu);
+                    ++step_done;
+                    cv_done.notify_all();
+                } else {
+                    push(&jb, (jb.h && jb.steps > 0) ? T_STEP : T_CLOSE);
+                }
+            } else if (t.kind == T_STEP) {
+                if (jb.h && jb.status == OGX_OK) step_job(jb, jb.h);
+                if (lockstep) {
+                    std::lock_guard<std::mutex> g(mu);
+                    ++step_done;
+                    cv_done.notify_all();
+                } else {
+                    push(&jb, (jb.status == OGX_OK && (int)jb.step_ms.size() < jb.steps) ? T_STEP : T_CLOSE);
+                }
+            } else {
+                if (jb.h) close_job(jb, jb.h);
+                jb.h = nullptr;
+                jb.t_done = now_s();
+                std::lock_guard<std::mutex> g(mu);
+                in_use -= jb.need_bytes;
+                --running;
+                ++finished;
+                cv_done.notify_all();
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    auto start_pool = [&]() {
+        for (int w = 0; w < workers; ++w) pool.emplace_back(worker);
+    };
+    auto stop_pool = [&]() {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            quit = true;
+        }
+        cv_work.notify_all();
+        for (auto& th : pool) th.join();
+        pool.clear();
+    };
+
+    if (ensemble && !solo) {
+        // lockstep ensemble: every system takes step s before any takes step s + 1
+        std::vector<Job*> live;
+        for (Job& jb : jobs) {
+            jb.need_bytes = footprint_bytes(jb.n, jb.p);
+            if (in_use + jb.need_bytes > budget) {
+                jb.rejected = true;
+                jb.status = OGX_ERR_INVALID;
+                ++rejected;
+                continue;
+            }
+            in_use += jb.need_bytes;
+            if (autotune) jb.thr = autotune_thr(jb, precision);
+            live.push_back(&jb);
+        }
+        const int L = (int)live.size();
+        lockstep = true;
+        start_pool();
+        auto round = [&](TaskKind k) {
+            {
+                std::lock_guard<std::mutex> g(mu);
+                step_done = 0;
+            }
+            for (Job* j : live) push(j, k);
+            std::unique_lock<std::mutex> lk(mu);
+            cv_done.wait(lk, [&]() { return step_done == L; });
+        };
+        round(T_OPEN);
+        std::vector<float> ens_ms;
+        const int S = smin;
+        const auto e0 = std::chrono::steady_clock::now();
+        for (int st = 0; st < S; ++st) {
+            const auto t0 = std::chrono::steady_clock::now();
+            round(T_STEP);
+            ens_ms.push_back((float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+        }
+        const double ens_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - e0).count();
+        lockstep = false;
+        running = L;
+        for (Job* j : live) push(j, T_CLOSE);
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_done.wait(lk, [&]() { return finished == L; });
+        }
+        stop_pool();
+        sampler.finish();
+        double bodysteps = 0.0;
+        int failed = 0;
+        std::vector<float> all;
+        for (const Job& jb : jobs) {
+            all.insert(all.end(), jb.step_ms.begin(), jb.step_ms.end());
+            bodysteps += (double)jb.n * (double)jb.step_ms.size();
+            if (jb.status != OGX_OK && !jb.rejected) ++failed;
+        }
+        std::printf("{\"mode\": \"ensemble\", \"precision\": \"%s\", \"jobs\": %d, \"failed\": %d, \"rejected\": %d, "
+                    "\"steps\": %zu, \"lockstep_steps\": %d, \"workers\": %d, \"wall_s\": %.3f, \"bodies_steps_per_s\": %.6e, "
+                    "\"ensemble_step_ms_p50\": %.3f, \"ensemble_step_ms_p99\": %.3f, \"p50_step_ms\": %.3f, "
+                    "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"autotune\": %s, \"warmup_s\": %.3f, "
+                    "\"jobs_detail\": [",
+                    precision == OGX_PREC_FP64 ? "fp64" : "mixed", njobs, failed, rejected, all.size(), S, workers, ens_s,
+                    bodysteps / ens_s, percentile(ens_ms, 0.5), percentile(ens_ms, 0.99), percentile(all, 0.5),
+                    percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s);
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            const Job& jb = jobs[j];
+            std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"kind\": \"%s\", \"status\": %d, "
+                        "\"rejected\": %s, \"step_ms_p50\": %.3f, \"digest\": \"%016llx\"}",
+                        j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.kind ? "disk+bulge merger" : "plummer",
+                        jb.status, jb.rejected ? "true" : "false", percentile(jb.step_ms, 0.5),
+                        (unsigned long long)jb.digest);
+        }
+        std::printf("]}\n");
+        return failed ? 1 : 0;
+    }
+
+    if (!solo) start_pool();
+    int admitted = 0;
     for (Job& jb : jobs) {
         jb.need_bytes = footprint_bytes(jb.n, jb.p);
         if (jb.need_bytes > budget) {
@@ -278,55 +512,70 @@ int main(int argc, char** argv) {
             ++rejected;
             continue;
         }
+        if (autotune) jb.thr = autotune_thr(jb, precision);
         if (solo) {
             sampler.peak = 0.0;
             sampler.armed = true;
             run_job(jb, precision);
             sampler.armed = false;
             jb.peak_bytes = std::max(0.0, sampler.peak.load() - idle);
+            jb.t_done = now_s();
             continue;
         }
         // wait for the arrival time, then for room under the budget
         const double wait = jb.arrival - now_s();
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
-        std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&]() { return running == 0 || in_use + jb.need_bytes <= budget; });
-        in_use += jb.need_bytes;
-        peak = std::max(peak, ++running);
-        lk.unlock();
-        threads.emplace_back([&, jp = &jb]() {
-            run_job(*jp, precision);
-            std::lock_guard<std::mutex> g(mu);
-            in_use -= jp->need_bytes;
-            --running;
-            cv.notify_all();
-        });
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_done.wait(lk, [&]() { return running == 0 || in_use + jb.need_bytes <= budget; });
+            in_use += jb.need_bytes;
+            peak = std::max(peak, ++running);
+        }
+        ++admitted;
+        push(&jb, T_OPEN);
     }
-    for (auto& th : threads) th.join();
+    if (!solo) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_done.wait(lk, [&]() { return finished == admitted; });
+        }
+        stop_pool();
+    }
     sampler.finish();
     const double wall = now_s();
-    std::vector<float> all;
-    double bodysteps = 0.0;
+    std::vector<float> all, turnaround;
+    double bodysteps = 0.0, step_s = 0.0;
     int failed = 0;
     for (const Job& jb : jobs) {
         all.insert(all.end(), jb.step_ms.begin(), jb.step_ms.end());
         bodysteps += (double)jb.n * (double)jb.step_ms.size();
+        for (float ms : jb.step_ms) step_s += ms * 1e-3;
         if (jb.status != OGX_OK && !jb.rejected) ++failed;
+        if (!jb.rejected && !solo) turnaround.push_back((float)(jb.t_done - jb.arrival));
     }
+    // wall_s runs from the first arrival to the last job's end and includes every
+    // job's set-up (initial conditions, first force evaluation) and, in served mode,
+    // the gaps between arrivals; the stepping-only figure divides by the summed step
+    // times instead (meaningful alone, where steps do not overlap)
     std::printf("{\"mode\": \"%s\", \"precision\": \"%s\", \"jobs\": %d, \"failed\": %d, \"rejected\": %d, "
-                "\"steps\": %zu, \"wall_s\": %.3f, \"bodies_steps_per_s\": %.6e, \"p50_step_ms\": %.3f, "
-                "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"jobs_detail\": [",
+                "\"steps\": %zu, \"workers\": %d, \"wall_s\": %.3f, \"warmup_s\": %.3f, \"bodies_steps_per_s\": %.6e, "
+                "\"stepping_only_bodies_steps_per_s\": %s, \"p50_step_ms\": %.3f, \"p99_step_ms\": %.3f, "
+                "\"job_turnaround_s_p50\": %s, \"job_turnaround_s_p99\": %s, "
+                "\"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"jobs_detail\": [",
                 solo ? "solo" : "served", precision == OGX_PREC_FP64 ? "fp64" : "mixed", njobs, failed, rejected,
-                all.size(), wall, bodysteps / wall, percentile(all, 0.5), percentile(all, 0.99), solo ? 1 : peak,
-                hbm_gb);
+                all.size(), solo ? 1 : workers, wall, warmup_s, bodysteps / wall,
+                solo ? std::to_string(step_s > 0 ? bodysteps / step_s : 0.0).c_str() : "null", percentile(all, 0.5),
+                percentile(all, 0.99), solo ? "null" : std::to_string(percentile(turnaround, 0.5)).c_str(),
+                solo ? "null" : std::to_string(percentile(turnaround, 0.99)).c_str(), solo ? 1 : peak, hbm_gb);
     for (size_t j = 0; j < jobs.size(); ++j) {
         const Job& jb = jobs[j];
-        std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"steps\": %d, \"kind\": \"%s\", \"status\": %d, "
-                    "\"rejected\": %s, \"need_mb\": %.1f, \"peak_mb\": %.1f, \"step_ms_p50\": %.3f, "
+        std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"steps\": %d, \"kind\": \"%s\", "
+                    "\"status\": %d, \"rejected\": %s, \"need_mb\": %.1f, \"peak_mb\": %.1f, \"step_ms_p50\": %.3f, "
                     "\"digest\": \"%016llx\"}",
-                    j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.steps, jb.kind ? "disk+bulge merger" : "plummer",
-                    jb.status, jb.rejected ? "true" : "false", jb.need_bytes / 1e6, jb.peak_bytes / 1e6,
-                    percentile(jb.step_ms, 0.5), (unsigned long long)jb.digest);
+                    j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.steps,
+                    jb.kind ? "disk+bulge merger" : "plummer", jb.status, jb.rejected ? "true" : "false",
+                    jb.need_bytes / 1e6, jb.peak_bytes / 1e6, percentile(jb.step_ms, 0.5),
+                    (unsigned long long)jb.digest);
     }
     std::printf("]}\n");
     return failed ? 1 : 0;

@@ -20,6 +20,8 @@
 // Potentials (pot = -G Phi) are produced alongside when requested.
 #include <algorithm>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "ogx_harmonics.cuh"
@@ -379,22 +381,35 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
 }
 
 // ---- mixed form ---------------------------------------------------------------------
-// host emulation of cvt.rna.tf32.f32 (round to nearest, ties away from zero)
 
 // Operator images for the tensor-core M2L, per offset o, column slice z, K-chunk c
 // and part (hi, lo): rows = the slice's output dofs (all of 1..K-1 when there is one
 // slice), K-major in the 128-byte-swizzle layout, exactly the bytes one pipeline
 // stage holds, so one bulk copy moves a chunk.
 // Also row 0 of every T_o (for the degree-0 local coefficient of potentials).
+struct MixedImages {
+    std::vector<uint8_t> img;
+    std::vector<double> row0;
+    std::vector<float> ounscale;
+};
+
+// built once per order in this process and shared by every handle
 template <int P>
-int ensure_mixed_tables(Handle& h) {
+std::shared_ptr<const MixedImages> mixed_images() {
     using C = mixed::TcCfg<P>;
-    if (h.mix_ready_p == P) return OGX_OK;
+    static std::mutex mu;
+    static std::shared_ptr<const MixedImages> cached;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached) return cached;
     const int K = C::K;
     std::vector<double> T((size_t)K * K);
-    std::vector<uint8_t> img((size_t)343 * C::NSPLIT * C::NCH * 2 * C::B_BYTES, 0);
-    std::vector<double> row0((size_t)343 * K, 0.0);
-    std::vector<float> ounscale(343, 0.f);
+    auto mi = std::make_shared<MixedImages>();
+    std::vector<uint8_t>& img = mi->img;
+    std::vector<double>& row0 = mi->row0;
+    std::vector<float>& ounscale = mi->ounscale;
+    img.assign((size_t)343 * C::NSPLIT * C::NCH * 2 * C::B_BYTES, 0);
+    row0.assign((size_t)343 * K, 0.0);
+    ounscale.assign(343, 0.f);
     for (int o = 0; o < 343; ++o) {
         const int ox = o % 7 - 3, oy = (o / 7) % 7 - 3, oz = o / 49 - 3;
         if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) <= 1) continue;
@@ -426,6 +441,17 @@ int ensure_mixed_tables(Handle& h) {
                 }
         }
     }
+    cached = mi;
+    return cached;
+}
+
+template <int P>
+int ensure_mixed_tables(Handle& h) {
+    if (h.mix_ready_p == P) return OGX_OK;
+    const auto mi = mixed_images<P>();
+    const std::vector<uint8_t>& img = mi->img;
+    const std::vector<double>& row0 = mi->row0;
+    const std::vector<float>& ounscale = mi->ounscale;
     uint8_t* d_img;
     double* d_row0;
     float* d_ous;

@@ -94,3 +94,24 @@ def test_fp64_jobs_give_the_same_bits_alone_and_in_the_mix():
     mixed = _serve(*args)
     assert solo["precision"] == mixed["precision"] == "fp64"
     assert [j["digest"] for j in solo["jobs_detail"]] == [j["digest"] for j in mixed["jobs_detail"]]
+
+
+ENS = ("--ensemble", "--steps", 4, "--jobs", 12, "--nmin", 8192, "--nmax", 131072, "--orders", "6,8", "--seed", 5)
+
+
+@pytest.mark.gpu
+def test_ensemble_members_match_their_solo_runs():
+    ens = _serve(*ENS)
+    solo = _serve(*ENS, "--solo")
+    assert ens["mode"] == "ensemble" and ens["failed"] == 0 and ens["peak_concurrent"] == 12
+    assert ens["steps"] == 12 * 4 == solo["steps"]
+    assert 0 < ens["ensemble_step_ms_p50"] <= ens["ensemble_step_ms_p99"]
+    assert [j["digest"] for j in ens["jobs_detail"]] == [j["digest"] for j in solo["jobs_detail"]]
+
+
+@pytest.mark.gpu
+def test_ensemble_autotune_picks_a_candidate_leaf_capacity():
+    out = _serve("--ensemble", "--steps", 2, "--jobs", 4, "--nmin", 8192, "--nmax", 65536, "--orders", "6,8",
+                 "--seed", 9, "--autotune")
+    assert out["failed"] == 0 and out["autotune"] is True
+    assert all(j["thr"] in (32, 48, 64, 96, 128) for j in out["jobs_detail"])
