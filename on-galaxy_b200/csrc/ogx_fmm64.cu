@@ -71,14 +71,14 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
     const size_t smem = mixed::far_smem_bytes<P>();
     const int lgrid = (tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, lblock = 32 * mixed::FAR_WARPS;
     if (pot) {
-        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32_heavy<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32_heavy<P, true>, (int)hsmem));
         mixed::k_leaf_far32_heavy<P, true><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
-        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32<P, true>, (int)smem));
         mixed::k_leaf_far32<P, true><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     } else {
-        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32_heavy<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32_heavy<P, false>, (int)hsmem));
         mixed::k_leaf_far32_heavy<P, false><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
-        OGX_CUDA(cudaFuncSetAttribute(mixed::k_leaf_far32<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32<P, false>, (int)smem));
         mixed::k_leaf_far32<P, false><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
     }
     return OGX_OK;
@@ -349,8 +349,8 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaEventRecord(h.ev[2], st));
     // upward
     const size_t p2x_smem = p2x_smem_bytes<P, double>();
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(smem_optin((const void*)k_p2x<P, 0, double>, (int)p2x_smem));
+    OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, double>, (int)p2x_smem));
     k_p2x<P, 0, double><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
     OGX_TRY(launch_m2m<P>(h, M));
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
@@ -358,7 +358,7 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
     if (h.ntgt > 0) {
         const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
-        OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
+        OGX_CUDA(smem_optin((const void*)k_m2l_fp64<P>, (int)m2l_smem));
         const int ntiles = h.ntgt_pad / M2L_TGT;
         k_m2l_fp64<P><<<ntiles, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M, Lown); ++h.launches;
     }
@@ -486,7 +486,7 @@ int run_mixed_upward(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
     OGX_TRY(arena_get(h.ws, S_MIX_MUNSCALE, (size_t)tv.nb, &mus));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(smem_optin((const void*)k_p2x<P, 0, float>, (int)p2x_smem));
     OGX_CUDA(cudaEventRecord(h.ev_tree, h.stream));
     const cudaStream_t main_st = h.stream, su = h.up;
     OGX_CUDA(cudaStreamWaitEvent(su, h.ev_tree, 0));
@@ -524,7 +524,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     double* nearb;
     OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
-    OGX_CUDA(cudaFuncSetAttribute(k_p2x<P, 1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2x_smem));
+    OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
     // join the upward pass
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
@@ -532,7 +532,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
     if (h.ntgt > 0) {
         if constexpr (C::SUPPORTED) {
-            OGX_CUDA(cudaFuncSetAttribute(mixed::k_m2l_tc<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+            OGX_CUDA(smem_optin((const void*)mixed::k_m2l_tc<P>, C::SMEM));
             mixed::k_m2l_tc<P><<<dim3(h.ntgt_pad / 128, C::NSPLIT), C::THREADS, C::SMEM, st>>>(
                 tv, h.tgt_tile_key, h.tgt_tile_box, mhi, mlo, mus, h.d_tc_img, h.d_tc_ounscale, Lown, h.d_err); ++h.launches;
             if (d_pot) {
@@ -542,7 +542,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         } else {
             // an order whose operand would not fit TMEM even in slices: the FP64 M2L serves it
             const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
-            OGX_CUDA(cudaFuncSetAttribute(k_m2l_fp64<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
+            OGX_CUDA(smem_optin((const void*)k_m2l_fp64<P>, (int)m2l_smem));
             k_m2l_fp64<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M,
                                                                            Lown); ++h.launches;
         }

@@ -22,6 +22,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -87,6 +89,23 @@ struct Arena {
     int get(Slot s, size_t bytes, void** out);
     void release();
 };
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (kernel, device) and size
+// in this process, not before every launch: the call costs host time, and a loop of
+// short launches (one per tree level) then waits on the host.
+inline cudaError_t smem_optin(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    int& cur = done[{func, dev}];
+    if (cur >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
 
 // Host-to-device copy of set-up data (operator tables) that has landed when this
 // returns.  cudaMemcpy from pageable host memory returns once the data is staged,

@@ -386,7 +386,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     level_off_dev = leafstart + n + 2;
     const size_t wm_smem = WM_BLOCK + thr + 16;
     if (wm_smem > 48 * 1024) {
-        OGX_CUDA(cudaFuncSetAttribute(k_topo_levels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wm_smem));
+        OGX_CUDA(smem_optin((const void*)k_topo_levels, (int)wm_smem));
     }
 
     // Leaves need the key order only down to their own level.  First attempt: sort
