@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, 
                                                           const int* __restrict__ child, const double* __restrict__ ctr,
                                                           const RootInfo* root, const int* __restrict__ col,
                                                           DevCounts* counts) {
+    __shared__ double s_kc[4][8][4];   // centres (x, y, z, half) of each warp's parent's children
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * 4 + wid;
     if (k >= count) return;
@@ -86,6 +87,11 @@ __global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, 
     int kids[8];
 #pragma unroll
     for (int t = 0; t < 8; ++t) kids[t] = child[8 * P + t];
+    if (lane < 32) {
+        const int t = lane >> 2, q = lane & 3;
+        s_kc[wid][t][q] = (kids[t] >= 0) ? ctr[4 * kids[t] + q] : 0.0;
+    }
+    __syncwarp();
     const double tol = root->tol;
     int mism = 0, nv = 0;
     if (lane < 27) {
@@ -96,6 +102,7 @@ __global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, 
             for (int s = 0; s < 8; ++s) {
                 const int c = child[8 * Q + s];
                 if (c < 0) continue;
+                const double cx = ctr[4 * c], cy = ctr[4 * c + 1], cz = ctr[4 * c + 2], ch = ctr[4 * c + 3];
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
                     const int b = kids[t];
@@ -103,7 +110,12 @@ __global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, 
                     const int ox = 2 * Dx + (s & 1) - (t & 1), oy = 2 * Dy + ((s >> 1) & 1) - ((t >> 1) & 1),
                               oz = 2 * Dz + ((s >> 2) & 1) - ((t >> 2) & 1);
                     const bool adj_i = max(abs(ox), max(abs(oy), abs(oz))) <= 1;
-                    if (adj_i != adjacent64(ctr, b, c, tol)) ++mism;
+                    // adjacent64(ctr, b, c, tol) with both centres already in hand
+                    const double* kb = s_kc[wid][t];
+                    const double lim = __dadd_rn(__dadd_rn(kb[3], ch), tol);
+                    const bool adj_f = fabs(__dsub_rn(kb[0], cx)) <= lim && fabs(__dsub_rn(kb[1], cy)) <= lim &&
+                                       fabs(__dsub_rn(kb[2], cz)) <= lim;
+                    if (adj_i != adj_f) ++mism;
                     if (adj_i) { if (col[27 * b + colleague_slot(ox, oy, oz)] != c) ++mism; }
                     else ++nv;
                 }
@@ -143,6 +155,13 @@ __global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restric
     if (lf >= nleaf) return;
     const int b = leafbox[lf];
     const double tol = root->tol;
+    // adjacent64(ctr, a, b, tol) with b's centre held in registers
+    const double bx = ctr[4 * b], by = ctr[4 * b + 1], bz = ctr[4 * b + 2], bh = ctr[4 * b + 3];
+    auto adj_b = [&](int a) {
+        const double lim = __dadd_rn(__dadd_rn(ctr[4 * a + 3], bh), tol);
+        return fabs(__dsub_rn(ctr[4 * a], bx)) <= lim && fabs(__dsub_rn(ctr[4 * a + 1], by)) <= lim &&
+               fabs(__dsub_rn(ctr[4 * a + 2], bz)) <= lim;
+    };
     int nu = 0, nw = 0;
     int64_t upairs = 0, ub = 0, wb = 0;
     bool overflow = false;
@@ -161,7 +180,7 @@ __global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restric
         if (c >= 0 && leafid[c] >= 0) addU(c);  // same-level adjacent leaves (b itself in slot 13)
         for (int A = parent[b]; A >= 0; A = parent[A]) {  // coarser adjacent leaves
             const int a2 = col[27 * A + d];
-            if (a2 >= 0 && leafid[a2] >= 0 && adjacent64(ctr, a2, b, tol)) addU(a2);
+            if (a2 >= 0 && leafid[a2] >= 0 && adj_b(a2)) addU(a2);
         }
         if (c >= 0 && c != b && leafid[c] < 0) {  // finer: descend the non-leaf colleague
             int stk[UW_STACK];
@@ -172,7 +191,7 @@ __global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restric
                 for (int s = 0; s < 8; ++s) {
                     const int ch = child[8 * node + s];
                     if (ch < 0) continue;
-                    if (!adjacent64(ctr, ch, b, tol)) {
+                    if (!adj_b(ch)) {
                         if (FILL) widx[wb + nw] = ch;
                         ++nw;
                     } else if (leafid[ch] >= 0) {
