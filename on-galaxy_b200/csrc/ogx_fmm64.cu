@@ -528,6 +528,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     // join the upward pass
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
+    // the near field needs only the tree and the lists: it may start with the M2L
+    OGX_CUDA(cudaEventRecord(h.ev_fork, st));
     // M2L on the tensor cores
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
     if (h.ntgt > 0) {
@@ -547,18 +549,18 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
                                                                            Lown); ++h.launches;
         }
     }
-    OGX_CUDA(cudaEventRecord(h.ev[4], st));
-    // near field on the low-priority side stream, after the M2L (which needs whole
-    // SMs): it fills what P2L, L2L and the far field leave idle
+    // near field on the low-priority side stream, launched after the M2L (which takes
+    // whole SMs first): its one-warp blocks fill what the M2L's tiles leave free, the
+    // SMs its last wave leaves idle, and then what P2L, L2L and the far field leave idle
     {
         const float eps2 = (float)(h.prm.eps * h.prm.eps);
-        OGX_CUDA(cudaEventRecord(h.ev_fork, st));
         OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
         const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
         if (d_pot) { mixed::k_leaf_near32<true><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
         else { mixed::k_leaf_near32<false><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
+    OGX_CUDA(cudaEventRecord(h.ev[4], st));
     if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }
     else { k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches; }
     OGX_CUDA(cudaEventRecord(h.ev[5], st));
