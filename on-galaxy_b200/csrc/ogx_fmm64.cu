@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
     if (any) {  // warp-uniform
         const double* T = opsT + (size_t)s * K * K;
         const int si = MODE == 0 ? s : 0;
-#pragma unroll 4
+#pragma unroll 8
         for (int kk = 0; kk < K; ++kk) {
             double tq[NPL];
 #pragma unroll
