@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp64rot"])
     ap.add_argument("--n-per", type=int, default=N_PER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -225,7 +225,7 @@ def main():
     # default stream has handle 0, which the library would replace by its own stream)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    prec = ogx.PREC_MIXED if args.precision == "mixed" else ogx.PREC_FP64
+    prec = {"mixed": ogx.PREC_MIXED, "fp64": ogx.PREC_FP64, "fp64rot": ogx.PREC_FP64_ROT}[args.precision]
     # ---- initial conditions (untimed): FP64 field for the circular velocities
     with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as ic_solver:
         pos, vel, mass, _ = ogx_ic.merger(args.n_per, seed=1, accel_fn=ic_solver.compute_accelerations)
@@ -333,7 +333,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "mixed(f32 P2P, scaled 3xFP16 tensor-core M2L, f64 translations)" if prec == ogx.PREC_MIXED else "f64",
+        "vs_baseline": None, "dtype": "mixed(f32 P2P, scaled 3xFP16 tensor-core M2L, f64 translations)" if prec == ogx.PREC_MIXED else ("f64 (rotation-based M2L)" if prec == ogx.PREC_FP64_ROT else "f64"),
         "data": "synthetic",
         "config": arm_config(n, args.n_per, world),
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),

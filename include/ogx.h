@@ -46,7 +46,11 @@ typedef enum {
 
 typedef enum {
     OGX_PREC_FP64 = 0,  /* plain form: FP64 end to end, matches AdaptiveFMM3D to <=1e-12 */
-    OGX_PREC_MIXED = 1  /* FP32 P2P + split-precision tensor-core M2L, FP64 upper translations */
+    OGX_PREC_MIXED = 1, /* FP32 P2P + split-precision tensor-core M2L, FP64 upper translations */
+    OGX_PREC_FP64_ROT = 2 /* third form, beyond the reference: FP64 end to end with the M2L factored into
+                           * rotation, z-axis translation and inverse rotation (O(p^3) per pair instead of
+                           * O(p^4)); equal to the plain form up to rounding, not to the reference's operation
+                           * order (README.md:75 of the reference defers this operator) */
 } ogx_precision;
 
 typedef struct {

@@ -185,8 +185,8 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     OGX_TRY(lists_build(h));
     OGX_CUDA(cudaEventRecord(h.ev[9], st));
     h.tree_valid = true;
-    if (h.prm.precision == OGX_PREC_FP64) OGX_TRY(fmm_fp64(h, d_acc, d_pot));
-    else OGX_TRY(fmm_mixed(h, d_acc, d_pot));
+    if (h.prm.precision == OGX_PREC_MIXED) OGX_TRY(fmm_mixed(h, d_acc, d_pot));
+    else OGX_TRY(fmm_fp64(h, d_acc, d_pot));   // the plain form, or with rotation-based M2L
     OGX_CUDA(cudaEventRecord(h.ev[8], st));
     const DevCounts& c = *h.h_counts;
     h.stats.num_boxes = (int32_t)c.num_boxes;
@@ -273,7 +273,8 @@ int ogx_create(const ogx_params* prm, void** handle) {
     *handle = nullptr;
     if (!(std::isfinite(prm->G)) || !(prm->eps >= 0.0) || !std::isfinite(prm->eps)) return OGX_ERR_INVALID;
     if (prm->solver != OGX_SOLVER_ADAPTIVE_FMM && prm->solver != OGX_SOLVER_DIRECT) return OGX_ERR_INVALID;
-    if (prm->precision != OGX_PREC_FP64 && prm->precision != OGX_PREC_MIXED) return OGX_ERR_INVALID;
+    if (prm->precision != OGX_PREC_FP64 && prm->precision != OGX_PREC_MIXED && prm->precision != OGX_PREC_FP64_ROT)
+        return OGX_ERR_INVALID;
     if (prm->solver == OGX_SOLVER_ADAPTIVE_FMM) {
         if (prm->p < 1 || prm->p > kPMax) return OGX_ERR_INVALID;
         if (prm->leaf_capacity < 1 || prm->leaf_capacity > 4096) return OGX_ERR_INVALID;
@@ -343,7 +344,9 @@ const char* ogx_name(void* handle) {
     if (!handle) return "ogx";
     HANDLE(handle);
     if (h.prm.solver == OGX_SOLVER_DIRECT) return "OgxDirect3D(B200, O(N^2) FP64)";
-    return h.prm.precision == OGX_PREC_FP64 ? "OgxAdaptiveFMM3D(B200, FP64)" : "OgxAdaptiveFMM3D(B200, mixed)";
+    return h.prm.precision == OGX_PREC_FP64       ? "OgxAdaptiveFMM3D(B200, FP64)"
+           : h.prm.precision == OGX_PREC_FP64_ROT ? "OgxAdaptiveFMM3D(B200, FP64, rotation M2L)"
+                                                  : "OgxAdaptiveFMM3D(B200, mixed)";
 }
 
 int ogx_eval_device(void* handle, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot) {

@@ -294,6 +294,164 @@ __global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uin
     }
 }
 
+// ---- M2L by rotations (the third form) ------------------------------------------------
+// T_o = Q_o^-1 Z_|o| Q_o (build_rot_pack): per tile of M2L_TGT targets sharing octant t
+// and per present (D, s) combination (offset o) the 64 source multipoles are staged,
+// then y = Q_o m (degree blocks) -> z = Z_|o| y (order blocks) -> acc += Q_o^-1 z
+// (degree blocks), the last sums kept in registers over all combinations.  Outputs are
+// laid out j-major (u = j * 64 + a), so a warp shares the dof j and its loop length and
+// reads each factor entry once for 32 sources.  FP64 throughout.
+template <int P>
+struct RotCfg {
+    static constexpr int K = (P + 1) * (P + 1);
+    static constexpr int LD = K | 1;
+    static constexpr int QSZ = (P + 1) * (2 * P + 1) * (2 * P + 3) / 3;   // sum_n (2n+1)^2
+    static constexpr int ZSZ = (P + 1) * (P + 2) * (2 * P + 3) / 6;       // sum_m (P+1-m)^2
+    static constexpr int PACK = 2 * QSZ + ZSZ;
+    static constexpr int NOUT = (M2L_TGT * K + M2L_THREADS - 1) / M2L_THREADS;
+    static constexpr size_t SMEM = (size_t)2 * M2L_TGT * LD * sizeof(double);
+};
+
+__device__ __forceinline__ int rot_degree(int j) {
+    int n = (int)sqrtf((float)j + 0.5f);
+    while (n * n > j) --n;
+    while ((n + 1) * (n + 1) <= j) ++n;
+    return n;
+}
+
+template <int P>
+__global__ void __launch_bounds__(M2L_THREADS) k_m2l_rot(TreeView tv, const uint32_t* tgt_key, const uint32_t* tgt_box,
+                                                        const double* __restrict__ pack, const double* __restrict__ mpole,
+                                                        double* lown) {
+    using R = RotCfg<P>;
+    constexpr int K = R::K, LD = R::LD;
+    extern __shared__ double s_rot[];
+    double* s_m = s_rot;                    // [64][LD] sources, later z
+    double* s_y = s_rot + M2L_TGT * LD;     // [64][LD] y = Q m
+    __shared__ int s_pcol[M2L_TGT][27];
+    __shared__ int s_src[M2L_TGT];
+    __shared__ int s_tgt[M2L_TGT];
+    __shared__ int s_t;
+    const int tid = threadIdx.x;
+    const int base = blockIdx.x * M2L_TGT;
+    if (tid == 0) s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
+    __syncthreads();
+    const int t = s_t;
+    if (t < 0) return;
+    if (tid < M2L_TGT) {
+        const int i = base + tid;
+        const int b = ((int)tgt_key[i] == t) ? (int)tgt_box[i] : -1;
+        s_tgt[tid] = b;
+        const int P_ = (b >= 0) ? tv.parent[b] : -1;
+        for (int d = 0; d < 27; ++d) s_pcol[tid][d] = (P_ >= 0) ? tv.col[27 * P_ + d] : -1;
+    }
+    __syncthreads();
+    const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
+    double acc[R::NOUT];
+#pragma unroll
+    for (int i = 0; i < R::NOUT; ++i) acc[i] = 0.0;
+    for (int D = 0; D < 27; ++D) {
+        const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+        for (int s = 0; s < 8; ++s) {
+            const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+            if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;  // adjacent: not in V
+            int mysrc = -1;
+            if (tid < M2L_TGT) {
+                const int Q = s_pcol[tid][D];
+                mysrc = (Q >= 0) ? tv.child[8 * Q + s] : -1;
+                s_src[tid] = mysrc;
+            }
+            if (!__syncthreads_or(mysrc >= 0)) continue;
+            for (int idx = tid; idx < M2L_TGT * K; idx += M2L_THREADS) {
+                const int r = idx / K, kk = idx - r * K;
+                const int src = s_src[r];
+                s_m[r * LD + kk] = (src >= 0) ? mpole[(size_t)src * K + kk] : 0.0;
+            }
+            __syncthreads();
+            const double* pk = pack + (size_t)((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) * R::PACK;
+            const double* Qf = pk;
+            const double* Qi = pk + R::QSZ;
+            const double* Zf = pk + 2 * R::QSZ;
+            // y = Q m, per degree block
+            for (int u = tid; u < M2L_TGT * K; u += M2L_THREADS) {
+                const int j = u / M2L_TGT, a = u - j * M2L_TGT;
+                const int n = rot_degree(j), w = 2 * n + 1, r = j - n * n;
+                const double* q = Qf + n * (2 * n - 1) * (2 * n + 1) / 3 + r * w;
+                const double* x = s_m + a * LD + n * n;
+                double v = 0.0;
+                for (int c = 0; c < w; ++c) v = fma(__ldg(q + c), x[c], v);
+                s_y[a * LD + j] = v;
+            }
+            __syncthreads();
+            // z = Z y, per order block (re and im parts share the block)
+            for (int u = tid; u < M2L_TGT * K; u += M2L_THREADS) {
+                const int j = u / M2L_TGT, a = u - j * M2L_TGT;
+                const int jd = rot_degree(j), r = j - jd * jd;
+                const int m = (r + 1) >> 1, part = (r == 0) ? 0 : ((r - 1) & 1);
+                const int w = P + 1 - m;
+                // zoff(m) = sum_{m' < m} (P+1-m')^2
+                const int zoff = R::ZSZ - w * (w + 1) * (2 * w + 1) / 6;
+                const double* z = Zf + zoff + (jd - m) * w;
+                const double* y = s_y + a * LD;
+                double v = 0.0;
+                for (int n = m; n <= P; ++n) v = fma(__ldg(z + (n - m)), y[m == 0 ? n * n : n * n + 2 * m - 1 + part], v);
+                s_m[a * LD + j] = v;
+            }
+            __syncthreads();
+            // acc += Q^-1 z
+#pragma unroll
+            for (int i = 0; i < R::NOUT; ++i) {
+                const int u = tid + i * M2L_THREADS;
+                if (u < M2L_TGT * K) {
+                    const int j = u / M2L_TGT, a = u - j * M2L_TGT;
+                    const int n = rot_degree(j), w = 2 * n + 1, r = j - n * n;
+                    const double* q = Qi + n * (2 * n - 1) * (2 * n + 1) / 3 + r * w;
+                    const double* x = s_m + a * LD + n * n;
+                    double v = acc[i];
+                    for (int c = 0; c < w; ++c) v = fma(__ldg(q + c), x[c], v);
+                    acc[i] = v;
+                }
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < R::NOUT; ++i) {
+        const int u = tid + i * M2L_THREADS;
+        if (u < M2L_TGT * K) {
+            const int j = u / M2L_TGT, a = u - j * M2L_TGT;
+            const int b = s_tgt[a];
+            if (b >= 0) lown[(size_t)b * K + j] += acc[i] / (2.0 * tv.center[4 * b + 3]);
+        }
+    }
+}
+
+// the 343 rotation packs of order P, built once per order in this process
+template <int P>
+std::shared_ptr<const std::vector<double>> rot_packs() {
+    static std::mutex mu;
+    static std::shared_ptr<const std::vector<double>> cached;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached) return cached;
+    auto v = std::make_shared<std::vector<double>>((size_t)343 * RotCfg<P>::PACK, 0.0);
+    for (int o = 0; o < 343; ++o) build_rot_pack(P, o, v->data() + (size_t)o * RotCfg<P>::PACK);
+    cached = v;
+    return cached;
+}
+
+template <int P>
+int ensure_rot_tables(Handle& h) {
+    if (h.rot_ready_p == P) return OGX_OK;
+    static_assert(RotCfg<P>::PACK > 0, "pack");
+    const auto pk = rot_packs<P>();
+    double* d;
+    OGX_TRY(arena_get(h.ws, S_ROT_PACK, pk->size(), &d));
+    OGX_CUDA(upload_now(d, pk->data(), pk->size() * sizeof(double)));
+    h.d_rot = d;
+    h.rot_ready_p = P;
+    return OGX_OK;
+}
+
 // ---- leaf near field (P2P over U) + final combine ----------------------------------------
 template <bool POT>
 __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot) {
@@ -356,7 +514,14 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(cudaEventRecord(h.ev[3], st));
     // M2L
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
-    if (h.ntgt > 0) {
+    if (h.ntgt > 0 && h.prm.precision == OGX_PREC_FP64_ROT) {
+        // third form: the same V pairs through the rotation-factored operators
+        OGX_TRY(ensure_rot_tables<P>(h));
+        constexpr size_t rsm = RotCfg<P>::SMEM;
+        OGX_CUDA(smem_optin((const void*)k_m2l_rot<P>, (int)rsm));
+        k_m2l_rot<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, rsm, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_rot, M, Lown);
+        ++h.launches;
+    } else if (h.ntgt > 0) {
         const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
         OGX_CUDA(smem_optin((const void*)k_m2l_fp64<P>, (int)m2l_smem));
         const int ntiles = h.ntgt_pad / M2L_TGT;

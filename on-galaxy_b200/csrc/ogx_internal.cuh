@@ -79,6 +79,7 @@ enum Slot {
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_MUNSCALE, S_MIX_OUNSCALE, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,
     S_NEAR32, S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
+    S_ROT_PACK,
     S_NUM_SLOTS
 };
 
@@ -212,6 +213,8 @@ struct Handle {
     bool tree_valid = false;
     // mixed-precision tables
     int mix_ready_p = -1;
+    int rot_ready_p = -1;          // order of the rotation-M2L factors in d_rot
+    double* d_rot = nullptr;       // rotation-M2L factors, 343 packs (build_rot_pack)
     uint8_t* d_tc_img = nullptr;   // tensor-core M2L operator images (hi/lo)
     double* d_tc_row0 = nullptr;   // row 0 of every M2L operator
     float* d_tc_ounscale = nullptr; // per M2L operator: 2^e undoing the scaling of its FP16 images
@@ -235,6 +238,10 @@ struct Handle {
 // kind 2: M2L for offset index (ox+3)+7(oy+3)+49(oz+3), source minus target in
 //         units of the box side; maps source M' -> target L' * side
 void build_operator(int kind, int p, int index, double* out /* K*K row-major */);
+void build_m2l_offset(int p, long double ox, long double oy, long double oz, double* out /* K*K */);
+// rotation-based M2L factors of V offset `index` (ogx_tables.cpp)
+int rot_pack_size(int p);
+bool build_rot_pack(int p, int index, double* out /* rot_pack_size(p) */);
 
 // ---- phases (defined in the .cu files) -------------------------------------
 int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);

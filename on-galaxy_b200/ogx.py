@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "libogx.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NO_DEVICE, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_STATE = range(8)
 SOLVER_ADAPTIVE_FMM, SOLVER_DIRECT = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_ROT = 0, 1, 2
 
 # Every entry point declared in include/ogx.h (checked by the ABI test).
 EXPORTS = (

@@ -113,3 +113,19 @@ def test_adjacent_offsets_have_no_m2l_matrix(ogx):
     assert np.all(ogx.operator_matrix(2, 4, 4 + 7 * 2 + 49 * 3) == 0.0)  # offset (1,-1,0)
     with pytest.raises(ogx.OgxError):
         ogx.operator_matrix(2, 4, 343)
+
+
+@pytest.mark.parametrize("p", [1, 2, 5, 8, 12])
+def test_rotation_factors_multiply_back_to_the_m2l_matrix(ogx, p):
+    """Kind 3 returns Q^-1 Z Q, the rotation-based form's factors of M2L offset o multiplied
+    out; it must equal the dense M2L matrix (kind 2) up to rounding, entry by entry."""
+    for idx in range(0, 343, 7):
+        ox, oy, oz = idx % 7 - 3, (idx // 7) % 7 - 3, idx // 49 - 3
+        T = ogx.operator_matrix(2, p, idx)
+        R = ogx.operator_matrix(3, p, idx)
+        if max(abs(ox), abs(oy), abs(oz)) <= 1:
+            assert not T.any() and not R.any()
+            continue
+        # each row's entries against that row's scale (rows of high degree are small)
+        scale = np.abs(T).max(axis=1, keepdims=True)
+        assert np.max(np.abs(R - T) / scale) <= 1e-13, (p, idx)
