@@ -633,7 +633,7 @@ int ensure_mixed_tables(Handle& h) {
     return OGX_OK;
 }
 
-// Mixed-form upward pass (P2M, M2M, TF32 split of the multipoles) on h.up, forked
+// Mixed-form upward pass (P2M, M2M, FP16 hi/lo split of the multipoles) on h.up, forked
 // from the main stream right after the tree build; the main stream joins it
 // (h.ev_up) before the M2L.
 template <int P>

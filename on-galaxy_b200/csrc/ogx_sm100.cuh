@@ -43,10 +43,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const 
     return false;
 }
 
-__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
-}
-// same, reading `bytes_valid` (0 or 16) bytes and zero-filling the rest
+// 16-byte cp.async reading `bytes_valid` (0 or 16) bytes and zero-filling the rest
 __device__ __forceinline__ void cp_async16_zfill(void* sdst, const void* gsrc, uint32_t bytes_valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes_valid)
                  : "memory");
@@ -77,17 +74,7 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows x 16 bytes,
-// `lbo` = byte distance between K-adjacent core matrices, `sbo` = between M/N-adjacent ones.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
-}
-// Same, 128-byte swizzle (layout type 2): rows of 128 bytes, 8-row atoms of 1024
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle (layout type 2): rows of 128 bytes, 8-row atoms of 1024
 // bytes `sbo` apart; the leading byte offset is unused for this layout (field 1).
 // The start address may advance inside the 128-byte line (K steps); the swizzle
 // is applied to absolute address bits, so the operand base must be 1024-aligned.
@@ -99,18 +86,6 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t sbo
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
     d |= (uint64_t)2 << 61;  // SWIZZLE_128B
     return d;
-}
-// Instruction descriptor: kind::tf32, D f32, A/B tf32, both K-major, dense.
-__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
-        : "memory");
 }
 // Instruction descriptor: kind::f16 with FP16 A/B, D f32, both K-major, dense.
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
@@ -136,20 +111,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
           "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
-// 32 lanes x 8 consecutive 32-bit columns
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-}
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// round-to-nearest fp32 -> tf32 (returned as an fp32 bit pattern with 13 low bits clear)
-__device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
 
 }  // namespace sm100
 }  // namespace ogx

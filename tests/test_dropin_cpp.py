@@ -46,5 +46,5 @@ def test_dropin_matches_reference_solvers(n, p, thr):
     assert out["verlet_max_rel"] <= 1e-12
     assert out["boxes_ogx"] == out["boxes_ref"]
     assert out["maxocc_ogx"] == out["maxocc_ref"]
-    # mixed form vs the reference FMM: FP32 near field / split-TF32 M2L rounding only
+    # mixed form vs the reference FMM: FP32 near field / split-FP16 M2L rounding only
     assert out["mixed_rms_rel"] <= 5e-6
