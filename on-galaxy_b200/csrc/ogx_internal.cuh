@@ -248,6 +248,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);
 int lists_build(Handle& h);
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
+int m2l_rot_launch(Handle& h, const double* M, double* Lown);   // third form's M2L, on h.stream
 int fmm_mixed_upward(Handle& h);   // upward pass on h.up, right after the tree (before the lists)
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
