@@ -160,9 +160,15 @@ __device__ __forceinline__ void for_regular(T x, T y, T z, F&& f) {
 template <int P, class T, class F>
 __device__ __forceinline__ void for_singular(T x, T y, T z, F&& f) {
     const T r2 = x * x + y * y + z * z;
-    const T ir2 = T(1) / r2;
+    T ir2, dr, di = 0;         // dr = S_0^0 = 1/rho
+    if constexpr (sizeof(T) == 4) {
+        dr = rsqrtf(r2);       // FP32 path: one rsqrt instead of a division and a square root
+        ir2 = dr * dr;
+    } else {
+        ir2 = T(1) / r2;
+        dr = sqrt(ir2);
+    }
     const T zr = z * ir2;      // FP32 path: one product per visit instead of two
-    T dr = sqrt(ir2), di = 0;  // S_0^0 = 1/rho
 #pragma unroll
     for (int m = 0; m <= P; ++m) {
         if (m > 0) {
