@@ -12,7 +12,7 @@
 // instead of the reference's O(N^2) pair sum, so they are available at any N.
 //
 // usage: ogx_galaxy_sim [--N n_per_galaxy] [--steps S] [--dt DT] [--stride F] [--p P]
-//                       [--thr T] [--eps E] [--seed S] [--precision fp64|mixed] [--out PREFIX]
+//                       [--thr T] [--eps E] [--seed S] [--precision fp64|fp64rot|mixed] [--out PREFIX]
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -51,7 +51,7 @@ int main(int argc, char** argv) {
         else if (a == "--thr") thr = std::atoi(v.c_str());
         else if (a == "--eps") eps = std::atof(v.c_str());
         else if (a == "--seed") seed = std::strtoull(v.c_str(), nullptr, 10);
-        else if (a == "--precision") precision = (v == "fp64") ? OGX_PREC_FP64 : OGX_PREC_MIXED;
+        else if (a == "--precision") precision = v == "fp64" ? OGX_PREC_FP64 : v == "fp64rot" ? OGX_PREC_FP64_ROT : OGX_PREC_MIXED;
         else if (a == "--out") out = v;
         else {
             std::fprintf(stderr, "unknown option %s\n", a.c_str());

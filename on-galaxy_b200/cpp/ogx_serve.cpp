@@ -271,7 +271,10 @@ int main(int argc, char** argv) {
         else if (a == "--thr") thr = std::atoi(next().c_str());
         else if (a == "--workers") workers = std::atoi(next().c_str());
         else if (a == "--steps") smin = smax = std::atoi(next().c_str());
-        else if (a == "--precision") precision = (next() == "fp64") ? OGX_PREC_FP64 : OGX_PREC_MIXED;
+        else if (a == "--precision") {
+            const std::string v = next();
+            precision = v == "fp64" ? OGX_PREC_FP64 : v == "fp64rot" ? OGX_PREC_FP64_ROT : OGX_PREC_MIXED;
+        }
         else if (a == "--orders") {
             orders.clear();
             std::string v = next();
@@ -486,7 +489,7 @@ int main(int argc, char** argv) {
                     "\"ensemble_step_ms_p50\": %.3f, \"ensemble_step_ms_p99\": %.3f, \"p50_step_ms\": %.3f, "
                     "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"autotune\": %s, \"warmup_s\": %.3f, "
                     "\"jobs_detail\": [",
-                    precision == OGX_PREC_FP64 ? "fp64" : "mixed", njobs, failed, rejected, all.size(), S, workers, ens_s,
+                    precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed", njobs, failed, rejected, all.size(), S, workers, ens_s,
                     bodysteps / ens_s, percentile(ens_ms, 0.5), percentile(ens_ms, 0.99), percentile(all, 0.5),
                     percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s);
         for (size_t j = 0; j < jobs.size(); ++j) {
@@ -562,7 +565,7 @@ int main(int argc, char** argv) {
                 "\"stepping_only_bodies_steps_per_s\": %s, \"p50_step_ms\": %.3f, \"p99_step_ms\": %.3f, "
                 "\"job_turnaround_s_p50\": %s, \"job_turnaround_s_p99\": %s, "
                 "\"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"jobs_detail\": [",
-                solo ? "solo" : "served", precision == OGX_PREC_FP64 ? "fp64" : "mixed", njobs, failed, rejected,
+                solo ? "solo" : "served", precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed", njobs, failed, rejected,
                 all.size(), solo ? 1 : workers, wall, warmup_s, bodysteps / wall,
                 solo ? std::to_string(step_s > 0 ? bodysteps / step_s : 0.0).c_str() : "null", percentile(all, 0.5),
                 percentile(all, 0.99), solo ? "null" : std::to_string(percentile(turnaround, 0.5)).c_str(),
