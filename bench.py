@@ -27,6 +27,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -43,18 +44,30 @@ THR = 64
 DT = 0.01
 
 
-# DRAM bytes per V-list pair of the tensor-core M2L launch (dram__bytes_read.sum +
-# dram__bytes_write.sum of k_m2l_tc<8> divided by the launch's V-list pairs), from the
-# ncu capture summarised in profiles/k_m2l_tc_merger500k.md; the bytes scale with the
-# pairs a launch processes (sources gathered per pair, results per target).
-M2L_DRAM_BYTES_PER_VPAIR = 15.13
+# DRAM bytes per V-list pair of the tensor-core M2L launch: dram__bytes_read.sum +
+# dram__bytes_write.sum of one k_m2l_tc<8> launch on the merger with 2 x 250,000 bodies
+# (ncu --set full --clock-control none), (50.96 + 2.90) MB over its 3.42e6 V-list pairs.
+# The bytes scale with the pairs a launch processes (sources gathered per pair, results
+# per target), so the figure is applied to the measured workload's pair count.
+M2L_DRAM_BYTES_PER_VPAIR = 15.74
 
 
 def arm_config(n, n_per, world):
-    """The workload both arms are quoted on (the reference arm times a bounded sample of it)."""
+    """The workload this arm is quoted on."""
     return {"workload": f"two-galaxy merger, {n} bodies (2x{n_per} disk+bulge), one leapfrog step dt=0.01",
             "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"replicas x{world}",
             "l2": "flushed (256 MiB write) before every timed step"}
+
+
+def reference_config(nsys, n_sys, n_per_full, world):
+    """What the reference arm runs per step: a bounded sample of the merger workload, `nsys`
+    independent mergers of n_sys bodies from the same generator, one per host thread (the
+    reference's AdaptiveFMM3D is single-threaded and takes minutes for one full-size merger)."""
+    return {"workload": f"{nsys} independent two-galaxy mergers of {n_sys} bodies each (2x{n_sys // 2} disk+bulge, "
+                        f"same generator as the {2 * n_per_full}-body merger), one AdaptiveFMM3D evaluation each "
+                        f"per step, one merger per host thread",
+            "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"{nsys} host threads",
+            "l2": "n/a (host)"}
 
 
 def max_over_ranks(x, dist, device):
@@ -127,7 +140,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "bodies/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": arm_config(2 * args.n_per, args.n_per, args.gpus),
+        "config": reference_config(threads, pos.shape[1], args.n_per, args.gpus),
         "p50_step_ms": 1e3 * float(np.percentile(times, 50)), "p99_step_ms": 1e3 * float(np.percentile(times, 99)),
         "cpu_baseline": {"value": value, "unit": "bodies/s", "cores": threads, "kind": kind,
                          "sample": f"{threads} independent {pos.shape[1]}-body mergers per step (same generator, "
@@ -161,8 +174,7 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.out = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/ogx_clocks_{os.getpid()}.csv"
+        self.out = os.path.join(tempfile.gettempdir(), f"ogx_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -202,6 +214,36 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- our arm
+def time_form(ogx, prec, p, pos, vel, mass, device, stream, flush, steps, warmup=2):
+    """Step time of one more form on the same workload, measured like the headline (device
+    resident, L2 flushed before every step, CUDA events on the library's stream)."""
+    import torch
+    with ogx.AdaptiveFMM3D(p=p, threshold=THR, precision=prec, device=device, stream=stream.cuda_stream) as s:
+        s.upload(pos, vel, mass)
+        for _ in range(warmup):
+            s.step(DT, 1)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s.step(DT, 1)
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        st = s.stats()
+    ms = np.array(ms)
+    return {"p": p, "ms_per_step": float(ms.mean()), "bodies_per_s": mass.shape[0] / (float(ms.mean()) / 1e3),
+            "p50_step_ms": float(np.percentile(ms, 50)), "p99_step_ms": float(np.percentile(ms, 99)),
+            "steps": steps, "ms_m2l": st["ms_m2l"], "ms_leaf": st["ms_leaf"]}
+
+
+def rms_max(ref, got):
+    a = np.linalg.norm(ref, axis=1)
+    e = np.linalg.norm(got - ref, axis=1)
+    return float(np.sqrt((e * e).sum() / (a * a).sum())), float(np.max(e / np.maximum(a, 1e-6 * a.max())))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -230,16 +272,8 @@ def main():
     with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as ic_solver:
         pos, vel, mass, _ = ogx_ic.merger(args.n_per, seed=1, accel_fn=ic_solver.compute_accelerations)
     n = mass.shape[0]
-    try:
-        solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local,
-                                   stream=stream.cuda_stream)
-        solver.upload(pos, vel, mass)
-    except ogx.OgxError as e:
-        if e.code != ogx.ERR_UNSUPPORTED:
-            raise
-        prec = ogx.PREC_FP64
-        solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local, stream=stream.cuda_stream)
-        solver.upload(pos, vel, mass)
+    solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local, stream=stream.cuda_stream)
+    solver.upload(pos, vel, mass)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -298,15 +332,34 @@ def main():
         with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as f64:
             acc64 = f64.compute_accelerations(pos, mass)
 
-        def errs(r, g):
-            a = np.linalg.norm(r, axis=1)
-            e = np.linalg.norm(g - r, axis=1)
-            return float(np.sqrt((e * e).sum() / (a * a).sum())), float(np.max(e / np.maximum(a, 1e-6 * a.max())))
-        rms, mx = errs(ref, acc_form)
-        rms64, mx64 = errs(ref, acc64)
-        rmsf, _ = errs(acc64, acc_form)
+        rms, mx = rms_max(ref, acc_form)
+        rms64, mx64 = rms_max(ref, acc64)
+        rmsf, _ = rms_max(acc64, acc_form)
         acc_info = {"rms_vs_fp64_direct": rms, "max_rel_vs_fp64_direct": mx, "rms_fp64_form_vs_direct": rms64,
                     "max_rel_fp64_form_vs_direct": mx64, "rms_vs_fp64_form": rmsf}
+
+    # ---- the other forms on the same workload, same process (untimed in the headline):
+    # the plain FP64 form at p = 8 (the mixed/plain speed-up), and both forms at p = 10,
+    # the lowest order whose truncation error against the FP64 direct sum is below 1e-5
+    forms = {}
+    if not args.no_accuracy and rank == 0 and prec == ogx.PREC_MIXED:
+        nf = max(3, min(args.steps, 5))
+        forms["fp64_p8"] = time_form(ogx, ogx.PREC_FP64, P_ORDER, pos, vel, mass, local, stream, flush, nf)
+        forms["fp64_p8"]["mixed_speedup"] = forms["fp64_p8"]["ms_per_step"] / ms_per_step
+        forms["mixed_p10"] = time_form(ogx, ogx.PREC_MIXED, 10, pos, vel, mass, local, stream, flush, nf)
+        forms["fp64_p10"] = time_form(ogx, ogx.PREC_FP64, 10, pos, vel, mass, local, stream, flush, nf)
+        forms["mixed_p10"]["mixed_speedup"] = forms["fp64_p10"]["ms_per_step"] / forms["mixed_p10"]["ms_per_step"]
+        with ogx.AdaptiveFMM3D(p=10, threshold=THR, precision=ogx.PREC_MIXED, device=local) as s10:
+            am10 = s10.compute_accelerations(pos, mass)
+        with ogx.AdaptiveFMM3D(p=10, threshold=THR, precision=ogx.PREC_FP64, device=local) as s10:
+            a6410 = s10.compute_accelerations(pos, mass)
+        r, m = rms_max(ref, am10)
+        forms["mixed_p10"].update({"rms_vs_fp64_direct": r, "max_rel_vs_fp64_direct": m,
+                                   "rms_vs_fp64_form": rms_max(a6410, am10)[0]})
+        r, m = rms_max(ref, a6410)
+        forms["fp64_p10"].update({"rms_vs_fp64_direct": r, "max_rel_vs_fp64_direct": m})
+        forms["note"] = ("same workload and timing as the headline (device-resident leapfrog step, L2 flushed); "
+                         "mixed_speedup = FP64-form step time / mixed-form step time at the same p")
 
     # ---- roofline of the dominant phase (CUDA events inside the library, same stream)
     phases = {k: float(np.mean([p[k] for p in phase])) for k in
@@ -342,7 +395,7 @@ def main():
         "phases_ms": phases, "tree": {k: st[k] for k in ("num_boxes", "num_leaves", "max_level", "max_leaf_occupancy",
                                                           "list_u", "list_v", "list_w", "p2p_pairs", "m2p_evals")},
         "pair_interactions_per_s": st["p2p_pairs"] * world / (ms_per_step / 1e3),
-        "roofline": roofline, "accuracy": acc_info, "clocks": clk.summary(),
+        "roofline": roofline, "accuracy": acc_info, "forms": forms, "clocks": clk.summary(),
         "gpu_launches": int(st.get("launches", 0)) * args.steps,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

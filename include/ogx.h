@@ -105,7 +105,8 @@ int ogx_synchronize(void* handle);
  * caller's other streams, and processes that reserve their device memory up front under a
  * fixed budget cannot have a library take more.  No handle is needed.
  * Host buffers: pos n*3 (Vec3 layout), mass n; out acc n*3, pot n or NULL; G and eps as in
- * KernelParams3D; stream is a cudaStream_t (NULL = the legacy default stream).  Bodies and
+ * KernelParams3D; stream is a cudaStream_t of the current device (NULL = the legacy default
+ * stream; a stream of another device returns OGX_ERR_INVALID).  Bodies and
  * results are staged in one fixed array that the library reserves on every GPU it is loaded
  * on: at most 65536 bodies (4 MiB, held until the process exits); larger n returns
  * OGX_ERR_INVALID.  The call returns when acc/pot hold the results.
@@ -121,6 +122,12 @@ int ogx_direct_eval_noalloc(int64_t n, const double* pos, const double* mass, do
 const char* ogx_name(void* handle);
 int ogx_last_stats(void* handle, ogx_stats* out);
 const char* ogx_strerror(int status);
+/* Diagnostic with no counterpart in the reference: runs the bounded device wait of the
+ * tensor-core M2L pipeline (an mbarrier wait that gives up after a poll limit and sets the
+ * handle's device error word) on a barrier that nothing arrives on, with `polls` (>= 1) as the
+ * limit.  Returns OGX_ERR_TIMEOUT, as an evaluation whose pipeline wait ran out does, and
+ * leaves the handle usable: the error word is cleared when it is reported. */
+int ogx_check_bounded_wait(void* handle, uint32_t polls);
 /* Text of the last error raised on the calling host thread (CUDA message etc.). */
 const char* ogx_last_error_message(void);
 /* Host-only helper (no GPU needed): the level-independent translation matrix used by the

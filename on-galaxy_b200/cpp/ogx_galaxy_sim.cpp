@@ -51,7 +51,15 @@ int main(int argc, char** argv) {
         else if (a == "--thr") thr = std::atoi(v.c_str());
         else if (a == "--eps") eps = std::atof(v.c_str());
         else if (a == "--seed") seed = std::strtoull(v.c_str(), nullptr, 10);
-        else if (a == "--precision") precision = v == "fp64" ? OGX_PREC_FP64 : v == "fp64rot" ? OGX_PREC_FP64_ROT : OGX_PREC_MIXED;
+        else if (a == "--precision") {
+            if (v == "fp64") precision = OGX_PREC_FP64;
+            else if (v == "fp64rot") precision = OGX_PREC_FP64_ROT;
+            else if (v == "mixed") precision = OGX_PREC_MIXED;
+            else {
+                std::fprintf(stderr, "unknown precision '%s' (expected fp64, fp64rot or mixed)\n", v.c_str());
+                return 2;
+            }
+        }
         else if (a == "--out") out = v;
         else {
             std::fprintf(stderr, "unknown option %s\n", a.c_str());

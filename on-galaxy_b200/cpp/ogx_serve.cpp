@@ -273,7 +273,13 @@ int main(int argc, char** argv) {
         else if (a == "--steps") smin = smax = std::atoi(next().c_str());
         else if (a == "--precision") {
             const std::string v = next();
-            precision = v == "fp64" ? OGX_PREC_FP64 : v == "fp64rot" ? OGX_PREC_FP64_ROT : OGX_PREC_MIXED;
+            if (v == "fp64") precision = OGX_PREC_FP64;
+            else if (v == "fp64rot") precision = OGX_PREC_FP64_ROT;
+            else if (v == "mixed") precision = OGX_PREC_MIXED;
+            else {
+                std::fprintf(stderr, "unknown precision '%s' (expected fp64, fp64rot or mixed)\n", v.c_str());
+                return 2;
+            }
         }
         else if (a == "--orders") {
             orders.clear();

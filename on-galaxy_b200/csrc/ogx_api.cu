@@ -17,6 +17,7 @@
 #include <mutex>
 
 #include "ogx_harmonics.cuh"
+#include "ogx_sm100.cuh"
 
 namespace ogx {
 
@@ -209,10 +210,22 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
 static int device_error(Handle& h) {
     if (h.h_err && *h.h_err) {
         *h.h_err = 0;
-        set_last_error(OGX_ERR_TIMEOUT, "a bounded device wait ran out (tensor-core M2L pipeline)");
+        set_last_error(OGX_ERR_TIMEOUT, "a bounded device wait ran out (mbarrier wait of the tensor-core M2L pipeline)");
         return OGX_ERR_TIMEOUT;
     }
     return OGX_OK;
+}
+
+// One thread waits, with the tensor-core pipeline's bounded wait and a limit of
+// `polls`, for phase 0 of an mbarrier that expects one arrival that never comes:
+// no copy and no MMA is outstanding, so the wait runs out and the error word is
+// set exactly as the M2L kernel sets it.
+__global__ void k_wait_probe(uint32_t polls, int* err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    sm100::mbar_init(&bar, 1);
+    sm100::fence_mbar_init();
+    if (!sm100::mbar_wait(&bar, 0, nullptr, polls)) atomicExch(err, 1);
 }
 
 static void finish_stats(Handle& h) {
@@ -604,6 +617,22 @@ int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx) {
     }
     off[nb] = e;
     return OGX_OK;
+}
+
+int ogx_check_bounded_wait(void* handle, uint32_t polls) {
+    if (!handle || polls == 0) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    DeviceGuard g(h.device);
+    DevCounts* dc;
+    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    h.d_err = &dc->kernel_error;
+    OGX_CUDA(cudaMemsetAsync(h.d_err, 0, sizeof(int), h.stream));
+    k_wait_probe<<<1, 32, 0, h.stream>>>(polls, h.d_err);
+    ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    return device_error(h);
 }
 
 }  // extern "C"

@@ -68,6 +68,19 @@ extern "C" int ogx_direct_eval_noalloc(int64_t n, const double* pos, const doubl
                                             " bodies");
         return OGX_ERR_INVALID;
     }
+    const cudaStream_t st = (cudaStream_t)stream;
+    if (st) {
+        // the staging array is looked up for the current device: a stream of another
+        // device would pair that device's work with this device's array
+        int sdev = -1, cur = -1;
+        OGX_CUDA(cudaStreamGetDevice(st, &sdev));
+        OGX_CUDA(cudaGetDevice(&cur));
+        if (sdev != cur) {
+            set_last_error(OGX_ERR_INVALID, "ogx_direct_eval_noalloc: the stream belongs to device " +
+                                                std::to_string(sdev) + ", the current device is " + std::to_string(cur));
+            return OGX_ERR_INVALID;
+        }
+    }
     double* base = nullptr;
     OGX_TRY(noalloc_scratch(&base));
     if (n == 0) return OGX_OK;
@@ -76,7 +89,6 @@ extern "C" int ogx_direct_eval_noalloc(int64_t n, const double* pos, const doubl
     double* d_mass = base + 3 * N;
     double* d_acc = base + 4 * N;
     double* d_pot = base + 7 * N;
-    const cudaStream_t st = (cudaStream_t)stream;
     // every staged input is overwritten in full and the kernel writes every output
     // it is asked for, so no part of the array has to start at zero
     OGX_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));

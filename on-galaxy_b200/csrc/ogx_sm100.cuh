@@ -33,9 +33,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait on phase `parity`; false = gave up (caller records the error)
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag) {
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+// bounded wait on phase `parity`; false = gave up after `limit` polls or when
+// *abort_flag became non-zero (the caller records the error)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag,
+                                          uint32_t limit = kSpinLimit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if (abort_flag && *abort_flag) return false;
         if (it > 32) __nanosleep(64);

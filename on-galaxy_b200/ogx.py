@@ -32,7 +32,7 @@ EXPORTS = (
     "ogx_name", "ogx_last_stats", "ogx_strerror", "ogx_last_error_message", "ogx_operator_matrix",
     "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
     "ogx_direct_eval_noalloc", "ogx_merger_params_default", "ogx_ic_merger", "ogx_set_species",
-    "ogx_diagnostics", "ogx_download_frame",
+    "ogx_diagnostics", "ogx_download_frame", "ogx_check_bounded_wait",
 )
 
 
@@ -112,6 +112,7 @@ def load(path: str = LIB_PATH):
     lib.ogx_set_species.argtypes = [vp, vp]
     lib.ogx_diagnostics.argtypes = [vp, dp]
     lib.ogx_download_frame.argtypes = [vp, vp]
+    lib.ogx_check_bounded_wait.argtypes = [vp, C.c_uint32]
     _lib = lib
     return lib
 
@@ -212,6 +213,11 @@ class _Solver:
 
     def synchronize(self):
         _check(self._lib.ogx_synchronize(self._h), "ogx_synchronize")
+
+    def check_bounded_wait(self, polls=1000):
+        """Run the pipeline's bounded device wait on a barrier nothing arrives on; raises
+        OgxError(ERR_TIMEOUT) as an evaluation whose wait ran out would."""
+        _check(self._lib.ogx_check_bounded_wait(self._h, int(polls)), "ogx_check_bounded_wait")
 
     def stats(self) -> dict:
         s = Stats()

@@ -25,8 +25,10 @@ stores inputs + outputs as .npz files:
                        gates) and the published convergence table
                        outputs/fmm3d_operator_convergence.csv
 
-Usage (needs /root/reference and `make -C oracle`):
-    python tests/golden/make_golden.py
+Usage (needs a checkout of the reference, found through the environment variable
+OGX_REFERENCE_DIR or else as a directory named `reference` beside this repository,
+and `make -C oracle`):
+    OGX_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -45,7 +47,8 @@ from oracle_lib import LISTS, Reference  # noqa: E402
 
 import ogx_ic  # noqa: E402
 
-REF_CSV = "/root/reference/outputs/fmm3d_operator_convergence.csv"
+REF_DIR = os.environ.get("OGX_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
+REF_CSV = os.path.join(REF_DIR, "outputs", "fmm3d_operator_convergence.csv")
 
 
 def tree_arrays(t, prefix):

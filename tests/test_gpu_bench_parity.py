@@ -1,0 +1,87 @@
+"""Parity at the benchmark's own sizes, against the reference and the pinned oracle.
+
+The bars of the smaller parity tests (test_gpu_fp64.py), taken to the configurations the
+benchmark and the accuracy numbers are quoted on:
+  * the 1M-body two-galaxy merger (the benchmark workload, leaf capacity 64) and the
+    262,144-body disk+bulge galaxy (leaf capacities 32, 64 and 128): the GPU octree and all
+    five interaction lists equal the reference's AdaptiveOctree (build + buildLists,
+    src3d/AdaptiveOctree.hpp:65-189) -- same boxes, centres bit for bit, same lists as sets,
+    the same bodies in every leaf in the same order;
+  * the 262,144-body galaxy at p = 4 and p = 8: the FP64 form matches the oracle, which is
+    bit-identical to the reference's AdaptiveFMM3D (src3d/AdaptiveFMM3D.hpp:29-110), to
+    max_rel <= 1e-12;
+  * the 1M merger: the GPU FP64 direct sum, which every accuracy figure of the benchmark is
+    measured against, matches a CPU FP64 direct sum (DirectSolver3D's formula,
+    src3d/DirectSolver3D.hpp:15-34) on 4,096 seeded targets to max_rel <= 1e-12.
+"""
+import numpy as np
+import pytest
+
+from helpers import assert_same_tree_arrays, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FMM_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def reference():
+    from oracle_lib import Reference
+    return Reference()
+
+
+@pytest.fixture(scope="module")
+def merger1m():
+    import ogx_ic
+    pos, _, mass, _ = ogx_ic.merger(500_000, seed=1, accel_fn=None)
+    return pos, mass
+
+
+@pytest.fixture(scope="module")
+def galaxy262k():
+    import ogx_ic
+    pos, mass, _ = ogx_ic.disk_bulge(262144, seed=11)
+    return pos, mass
+
+
+def _gpu_tree(ogx, pos, mass, thr):
+    with ogx.AdaptiveFMM3D(p=2, threshold=thr, precision=ogx.PREC_FP64) as s:
+        s.compute_accelerations(pos, mass)
+        st = s.stats()
+        return s.tree(), st
+
+
+def test_merger_1m_tree_and_lists_match_reference(ogx, reference, merger1m):
+    pos, mass = merger1m
+    t, st = _gpu_tree(ogx, pos, mass, 64)
+    assert st["adjacency_mismatch"] == 0
+    assert_same_tree_arrays(t, reference.tree(pos, 64), "merger 1M thr 64")
+
+
+@pytest.mark.parametrize("thr", [32, 64, 128])
+def test_galaxy_262k_tree_and_lists_match_reference(ogx, reference, galaxy262k, thr):
+    pos, mass = galaxy262k
+    t, st = _gpu_tree(ogx, pos, mass, thr)
+    assert st["adjacency_mismatch"] == 0 and st["max_leaf_occupancy"] <= thr
+    assert_same_tree_arrays(t, reference.tree(pos, thr), f"galaxy 262k thr {thr}")
+
+
+@pytest.mark.parametrize("p", [4, 8])
+def test_galaxy_262k_fp64_form_matches_oracle(ogx, oracle, galaxy262k, p):
+    pos, mass = galaxy262k
+    with ogx.AdaptiveFMM3D(p=p, threshold=64, precision=ogx.PREC_FP64) as s:
+        acc = s.compute_accelerations(pos, mass)
+    ref = oracle.adaptive_fmm(pos, mass, p=p, thr=64, with_pot=False)
+    mx, rms = rel_err(ref, acc)
+    assert mx <= FMM_TOL, (p, mx, rms)
+
+
+def test_merger_1m_direct_sum_matches_cpu_on_seeded_targets(ogx, oracle, merger1m):
+    pos, mass = merger1m
+    with ogx.DirectSolver3D() as d:
+        acc, pot = d.compute_accelerations(pos, mass, with_potential=True)
+    idx = np.sort(np.random.default_rng(2024).choice(mass.shape[0], 4096, replace=False)).astype(np.int64)
+    ref_acc, ref_pot = oracle.direct_targets(pos, mass, idx)
+    mx, _ = rel_err(ref_acc, acc[idx])
+    assert mx <= 1e-12, mx
+    assert np.max(np.abs(pot[idx] - ref_pot) / np.abs(ref_pot)) <= 1e-12

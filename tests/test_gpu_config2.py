@@ -4,8 +4,9 @@
 The CPU oracle cannot run this size in seconds, so the checks are size-independent:
   * the FP64 form converges with p against the GPU FP64 direct sum (itself equal to
     DirectSolver3D to 1e-12, see test_gpu_fp64.py), with RMS errors at the level the
-    reference's operators reach (1.3e-3 / 1.3e-5 / 5e-7 at p = 4 / 8 / 12 on
-    a Plummer sphere);
+    reference's own AdaptiveFMM3D reaches against DirectSolver3D (1.3e-3 / 1.3e-5 / 5e-7
+    at p = 4 / 8 / 12 on a 16,384-body Plummer sphere, measured with the reference built
+    from its src3d headers);
   * the mixed form stays within the mixed tolerance of the FP64 form at every p and
     leaf capacity (it must not add error on top of the truncation error);
   * trees are consistent: every body in exactly one leaf, no leaf above capacity unless

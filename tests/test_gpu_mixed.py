@@ -65,3 +65,19 @@ def test_mixed_leapfrog_runs_and_tracks_fp64(ogx, golden):
             out.append(s.download())
     np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-9)
     assert rel_err(out[0][2], out[1][2])[1] <= 5e-6
+
+
+def test_bounded_wait_runs_out_and_the_handle_stays_usable(ogx, golden):
+    """The tensor-core pipeline's bounded mbarrier wait, given a barrier nothing arrives on,
+    gives up after its poll limit and the host reports OGX_ERR_TIMEOUT (no copy or MMA is
+    outstanding, so no GPU fault is involved); the same handle then evaluates as before."""
+    d = golden("plummer2000_s2")
+    with ogx.AdaptiveFMM3D(p=8, threshold=64, precision=ogx.PREC_MIXED) as s:
+        a1 = s.compute_accelerations(d["pos"], d["mass"])
+        for polls in (1, 1000):
+            with pytest.raises(ogx.OgxError) as e:
+                s.check_bounded_wait(polls)
+            assert e.value.code == ogx.ERR_TIMEOUT
+            s.synchronize()   # the error word was cleared when it was reported
+        a2 = s.compute_accelerations(d["pos"], d["mass"])
+    np.testing.assert_array_equal(a1, a2)

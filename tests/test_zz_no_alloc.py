@@ -53,3 +53,19 @@ def test_noalloc_matches_direct_solver_on_consecutive_calls(ogx):
         assert _max_rel(ref_acc, acc) <= DIRECT_TOL
         if with_pot:
             assert _max_rel(ref_pot, pot) <= DIRECT_TOL
+
+
+@pytest.mark.gpu
+def test_noalloc_on_a_caller_stream(ogx):
+    """A caller's own (non-default) stream is honoured: the call returns with the results in
+    place, twice in a row on the same stream."""
+    import torch
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    for seed in (4, 5):
+        pos, mass = _bodies(7000, seed)
+        with ogx.DirectSolver3D(G=1.0, eps=0.0) as d:
+            ref_acc = d.compute_accelerations(pos, mass)
+        acc = ogx.direct_eval_noalloc(pos, mass, G=1.0, eps=0.0, stream=stream.cuda_stream)
+        assert _max_rel(ref_acc, acc) <= DIRECT_TOL
