@@ -21,13 +21,18 @@
 //     the result is drained;
 //   * accumulation: FP32 accumulation over all ~6000 MMA steps of a tile loses
 //     ~1e-5 of the (strongly cancelling) far field, so every combination gets a
-//     fresh FP32 accumulator (two ping-pong buffers in TMEM) that the epilogue
-//     warps drain into an FP64 accumulator also kept in TMEM (two 32-bit
-//     columns per value) while the MMA warp proceeds with the next combination;
+//     fresh FP32 accumulator (a ring of buffers in TMEM) that the epilogue warps
+//     drain while the MMA warp proceeds with the next combination.  The drain
+//     unscales each combination's result, sums the (at most eight) combinations
+//     of one colleague slot D in FP32 registers, and folds each slot's sum into
+//     an FP64 accumulator (registers for p <= 8, TMEM otherwise);
 //   * operands: K is cut into chunks of 64 fp16 (one 128-byte line per row) in
 //     the K-major 128-byte-swizzle layout; A rows are gathered with cp.async,
 //     each T_o chunk is a pre-laid-out image copied by the TMA bulk engine
-//     (cp.async.bulk, no multicast); up to 4 stages pipeline through mbarriers;
+//     (cp.async.bulk, no multicast); up to 4 stages pipeline through mbarriers.
+//     A producer thread hands its rows of a stage over with an asynchronous
+//     mbarrier arrival that fires when its copies have landed, so it never waits
+//     for its own copies and every stage of the ring can be in flight;
 //   * warp specialisation: four warps gather the A rows (the colleague table
 //     of the tile is staged in shared memory and the next combination's source
 //     index is fetched one combination ahead), one lane issues the MMAs, and
@@ -169,8 +174,6 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
     using C = TcCfg<P>;
     static_assert(C::SUPPORTED, "tensor-core M2L: operand does not fit");
     const int zs = blockIdx.y;                    // output column slice
-    // gathers kept in flight per producer thread before its row is handed to the MMA
-    constexpr int LAG = C::STAGES >= 4 ? C::STAGES - 2 : 1;
     constexpr int NG = C::NPAD / 16;
     constexpr int NGRP = C::NGRP;
     constexpr int NBUF = C::NBUF;
@@ -183,7 +186,9 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
     __shared__ int s_t, s_ncombo;
     __shared__ int s_box[128];
     __shared__ int s_Q[27][128];      // colleague slot D of each target's parent
-    __shared__ uint32_t s_mask[6];
+    __shared__ int s_par[128];
+    __shared__ uint32_t s_mask[7];    // bit D * 8 + s: some target of the tile has that V source
+    __shared__ int s_wcnt[7];
     __shared__ int s_combo[189];      // present combinations: D | s << 5 | o << 8
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int base = blockIdx.x * 128;
@@ -202,61 +207,109 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
         sm100::mbar_init(&fin, 1);
         sm100::fence_mbar_init();
     }
-    if (tid < 6) s_mask[tid] = 0;
+    if (tid < 7) s_mask[tid] = 0;
     __syncthreads();
     const int t = s_t;
     if (t < 0) return;
+    // the A operands of every stage start at zero (rows without a source are not copied)
+    for (int i = tid; i < C::STAGES * 2 * C::A_BYTES / 16; i += blockDim.x) {
+        const int sg = i / (2 * C::A_BYTES / 16), off = i - sg * (2 * C::A_BYTES / 16);
+        reinterpret_cast<uint4*>(smem + (size_t)sg * C::STAGE_BYTES)[off] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    sm100::fence_proxy_async();
     const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
     if (warp == 4) sm100::tmem_alloc(&s_tmem, C::TMEM_COLS);
     if (tid < 128) {
         const uint32_t key = tgt_key[base + tid];
         const int myb = (key == (uint32_t)t) ? (int)tgt_box[base + tid] : -1;
         s_box[tid] = myb;
-        const int par = (myb >= 0) ? tv.parent[myb] : -1;
-#pragma unroll 9
-        for (int D = 0; D < 27; ++D) s_Q[D][tid] = (par >= 0) ? tv.col[27 * par + D] : -1;
+        s_par[tid] = (myb >= 0) ? tv.parent[myb] : -1;
     }
     __syncthreads();
-    // presence mask over the 189 (D, s) combinations of octant t
-    if (tid < 128) {
-        int ci = 0;
-        for (int D = 0; D < 27; ++D) {
-            const int Q = s_Q[D][tid];
-            int ch[8];
-            if (Q >= 0) {
-                const int4 c0 = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Q));
-                const int4 c1 = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Q) + 1);
-                ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
-                ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
-            } else {
+    // Colleague slots and the children they offer, spread over the whole CTA: thread
+    // (group g, row r) takes slots D = g, g + NGS, ... of target r, with all its loads
+    // in flight together.  A warp holds one g and 32 targets, so one OR over the warp
+    // gives the presence bits of its slots.
+    {
+        constexpr int NGS = C::THREADS / 128;
+        constexpr int DPT = (27 + NGS - 1) / NGS;
+        constexpr int NW = (DPT * 8 + 31) / 32;
+        const int r = tid & 127, g = tid >> 7;
+        if (g < NGS) {
+            const int par = s_par[r];
+            int Qv[DPT];
 #pragma unroll
-                for (int s = 0; s < 8; ++s) ch[s] = -1;
+            for (int i = 0; i < DPT; ++i) {
+                const int D = g + i * NGS;
+                Qv[i] = (D < 27 && par >= 0) ? __ldg(tv.col + 27 * (size_t)par + D) : -1;
             }
-            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+            int4 cr[DPT][2];
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
-                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
-                const unsigned bal = __ballot_sync(0xffffffffu, ch[s] >= 0);
-                if (lane == 0 && bal) atomicOr(&s_mask[ci >> 5], 1u << (ci & 31));
-                ++ci;
+            for (int i = 0; i < DPT; ++i) {
+                const int D = g + i * NGS;
+                if (D < 27) s_Q[D][r] = Qv[i];
+                if (Qv[i] >= 0) {
+                    cr[i][0] = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Qv[i]));
+                    cr[i][1] = __ldg(reinterpret_cast<const int4*>(tv.child + 8 * (size_t)Qv[i]) + 1);
+                } else {
+                    cr[i][0] = cr[i][1] = make_int4(-1, -1, -1, -1);
+                }
+            }
+            uint32_t bw[NW];
+#pragma unroll
+            for (int w = 0; w < NW; ++w) bw[w] = 0;
+#pragma unroll
+            for (int i = 0; i < DPT; ++i) {
+                const int D = g + i * NGS;
+                const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
+                const int ch[8] = {cr[i][0].x, cr[i][0].y, cr[i][0].z, cr[i][0].w,
+                                   cr[i][1].x, cr[i][1].y, cr[i][1].z, cr[i][1].w};
+#pragma unroll
+                for (int s = 0; s < 8; ++s) {
+                    const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
+                    if (D < 27 && max(abs(ox), max(abs(oy), abs(oz))) > 1 && ch[s] >= 0) bw[i >> 2] |= 1u << (8 * (i & 3) + s);
+                }
+            }
+#pragma unroll
+            for (int w = 0; w < NW; ++w) bw[w] = __reduce_or_sync(0xffffffffu, bw[w]);
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i < DPT; ++i) {
+                    const int D = g + i * NGS;
+                    const uint32_t byte = (bw[i >> 2] >> (8 * (i & 3))) & 0xFFu;
+                    if (D < 27 && byte) atomicOr(&s_mask[D >> 2], byte << (8 * (D & 3)));
+                }
             }
         }
     }
     __syncthreads();
-    if (tid == 0) {
-        int n = 0, ci = 0;
-        for (int D = 0; D < 27; ++D) {
-            const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
-            for (int s = 0; s < 8; ++s) {
+    // the present combinations in (D, s) order, placed by a ballot prefix over 7 warps
+    {
+        bool pres = false;
+        int code = 0;
+        unsigned bal = 0;
+        if (tid < 224) {
+            const int c = tid, D = c >> 3, s = c & 7;
+            if (c < 216 && ((s_mask[c >> 5] >> (c & 31)) & 1u)) {
+                const int Dx = D % 3 - 1, Dy = (D / 3) % 3 - 1, Dz = D / 9 - 1;
                 const int ox = 2 * Dx + (s & 1) - tx, oy = 2 * Dy + ((s >> 1) & 1) - ty, oz = 2 * Dz + ((s >> 2) & 1) - tz;
-                if (max(abs(ox), max(abs(oy), abs(oz))) <= 1) continue;
-                if ((s_mask[ci >> 5] >> (ci & 31)) & 1u)
-                    s_combo[n++] = D | (s << 5) | (((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) << 8);
-                ++ci;
+                pres = true;
+                code = D | (s << 5) | (((ox + 3) + 7 * (oy + 3) + 49 * (oz + 3)) << 8);
             }
+            bal = __ballot_sync(0xffffffffu, pres);
+            if (lane == 0) s_wcnt[warp] = __popc(bal);
         }
-        s_ncombo = n;
+        __syncthreads();
+        if (pres) {
+            int pos = __popc(bal & ((1u << lane) - 1u));
+            for (int w = 0; w < warp; ++w) pos += s_wcnt[w];
+            s_combo[pos] = code;
+        }
+        if (tid == 0) {
+            int n = 0;
+            for (int w = 0; w < 7; ++w) n += s_wcnt[w];
+            s_ncombo = n;
+        }
     }
     sm100::tc_fence_before();
     __syncthreads();
@@ -295,6 +348,9 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                         atomicExch(err, 1);
                         break;
                     }
+                    // the A rows were written by cp.async (generic proxy); the MMA reads
+                    // them through the async proxy
+                    sm100::fence_proxy_async();
                     sm100::tc_fence_after();
                     const uint64_t ds = desc0 + (uint64_t)(s * D_STAGE);
                     const int nks = min(C::CH, C::NKS - c * C::CH);
@@ -379,23 +435,21 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                     const int q = (i & 1) * 4 + (lane >> 3);          // 16-byte piece (8 fp16) of the chunk
                     const int rs = __shfl_sync(0xffffffffu, src, rl);
                     if (q < nq) {
-                        const __half* g = (part ? mlo : mhi) + (size_t)max(rs, 0) * C::KPAD + k0 + 8 * q;
-                        sm100::cp_async16_zfill(st + part * C::A_BYTES + tile_off(32 * warp + rl, 8 * q), g,
-                                                rs >= 0 ? 16u : 0u);
+                        // an absent source leaves the row's previous contents (finite
+                        // values of an earlier row, or the zeros written at start): the
+                        // drain multiplies that row's result by an unscale of 0
+                        if (rs >= 0)
+                            sm100::cp_async16(st + part * C::A_BYTES + tile_off(32 * warp + rl, 8 * q),
+                                              (part ? mlo : mhi) + (size_t)rs * C::KPAD + k0 + 8 * q);
                     }
                 }
-                sm100::cp_async_commit();
-                if (u >= LAG) {
-                    sm100::cp_async_wait<LAG>();
-                    sm100::fence_proxy_async();
-                    sm100::mbar_arrive(&afull[(u - LAG) % C::STAGES]);
-                }
+                // the stage's A barrier counts one arrival per producer thread, made
+                // when that thread's copies have landed: the producer moves on at once,
+                // so every stage of the ring can have its gathers in flight
+                sm100::cp_async_mbar_arrive_noinc(&afull[s]);
             }
         }
-        sm100::cp_async_wait<0>();
-        sm100::fence_proxy_async();
-        if (!s_abort)
-            for (int v = max(0, u - LAG); v < u; ++v) sm100::mbar_arrive(&afull[v % C::STAGES]);
+        sm100::cp_async_wait_all();
         if (s_abort && r == 0) {
             // let this thread's bulk copies land before the CTA exits
             for (int s = 0; s < C::STAGES; ++s)
@@ -409,14 +463,19 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
         const uint32_t tmem_lane = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;
         double racc[C::REGACC ? C::MAXG : 1][16];
+        float part[C::REGACC ? C::MAXG : 1][16];
 #pragma unroll
         for (int g = 0; g < (C::REGACC ? C::MAXG : 1); ++g)
 #pragma unroll
-            for (int i = 0; i < 16; ++i) racc[g][i] = 0.0;
+            for (int i = 0; i < 16; ++i) racc[g][i] = 0.0, part[g][i] = 0.f;
         for (int k = 0; k < nco && !s_abort; ++k) {
             const int a = k % NBUF;
             // this row's source for combination k and the scales its operands carry
             const int code = s_combo[k];
+            // combinations come grouped by colleague slot D (the eight children of one
+            // colleague, at similar distances): their FP32 results are summed in FP32 and
+            // the slot's sum is folded into FP64 once, after its last combination
+            const bool fold = (k + 1 == nco) || ((s_combo[k + 1] & 31) != (code & 31));
             const int Q = s_Q[code & 31][row];
             const int srcb = (Q >= 0) ? __ldg(tv.child + 8 * (size_t)Q + ((code >> 5) & 7)) : -1;
             const float unscale = (srcb >= 0) ? __ldg(munscale + srcb) * __ldg(ounscale + (code >> 8)) : 0.f;
@@ -431,15 +490,26 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
                 for (int g = 0; g < C::MAXG; ++g) {
                     const int c16 = g0 + g;
                     if (c16 < g1) {
-                        uint32_t v[16], w[16];
-                        sm100::tmem_ld16(tmem_lane + a * C::DBUF + c16 * 16, v);
-                        sm100::tmem_ld16(tmem_lane + a * C::DBUF + C::NPAD + c16 * 16, w);
-                        sm100::tmem_ld_wait();
-                        // the two partial products meet in FP32 (w is ~2^-11 of v), then one
-                        // conversion and one FP64 add per column: the FP64 pipe bounds the drain
+                        // two halves of 8 columns keep the drain's registers within the
+                        // launch's budget; the two partial products meet in FP32 (w is
+                        // ~2^-11 of v)
 #pragma unroll
-                        for (int i = 0; i < 16; ++i)
-                            racc[g][i] += (double)((__uint_as_float(v[i]) + __uint_as_float(w[i])) * unscale);
+                        for (int h = 0; h < 2; ++h) {
+                            uint32_t v[8], w[8];
+                            sm100::tmem_ld8(tmem_lane + a * C::DBUF + c16 * 16 + 8 * h, v);
+                            sm100::tmem_ld8(tmem_lane + a * C::DBUF + C::NPAD + c16 * 16 + 8 * h, w);
+                            sm100::tmem_ld_wait();
+#pragma unroll
+                            for (int i = 0; i < 8; ++i)
+                                part[g][8 * h + i] = fmaf(__uint_as_float(v[i]) + __uint_as_float(w[i]), unscale, part[g][8 * h + i]);
+                        }
+                        if (fold) {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) {
+                                racc[g][i] += (double)part[g][i];
+                                part[g][i] = 0.f;
+                            }
+                        }
                     }
                 }
             } else {
