@@ -557,10 +557,13 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     // SMs its last wave leaves idle, and then what P2L, L2L and the far field leave idle
     {
         const float eps2 = (float)(h.prm.eps * h.prm.eps);
+        float4* rel;
+        OGX_TRY(arena_get(h.ws, S_MIX_POS4, 2 * (size_t)tv.n, &rel));
         OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
+        mixed::k_near_prep<<<(tv.n + 255) / 256, 256, 0, h.side>>>(tv, rel, rel + tv.n); ++h.launches;
         const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
-        if (d_pot) { mixed::k_leaf_near32<true><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
-        else { mixed::k_leaf_near32<false><<<ngrid, 32, 0, h.side>>>(tv, eps2, nearb); ++h.launches; }
+        if (d_pot) { mixed::k_leaf_near32<true><<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches; }
+        else { mixed::k_leaf_near32<false><<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches; }
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));

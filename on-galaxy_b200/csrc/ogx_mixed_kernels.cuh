@@ -621,11 +621,13 @@ __global__ void __launch_bounds__(128) k_m2l_dof0(TreeView tv, int ntgt_pad, con
 }
 
 // ---- FP32 near field ------------------------------------------------------------
-// Leaf-centred double-float positions: every coordinate relative to the target
-// leaf centre is held as hi + lo FP32 (hi = fp32(x - c), lo = fp32((x - c) - hi),
-// the shift taken in FP64), so d = (s_hi - t_hi) + (s_lo - t_lo) carries the
-// FP32 relative accuracy of |d| itself even for very close pairs.  Sources of each
-// U-list entry are staged (re-centred) in shared memory once per target leaf.
+// Double-float coordinates: every sorted body's position relative to the root centre
+// is held as hi + lo FP32 (hi = fp32(x - c), lo = fp32((x - c) - hi), the difference
+// taken in FP64; k_near_prep, once per evaluation).  For a close pair the two hi parts
+// lie within a factor of two of each other, so s_hi - t_hi is exact (Sterbenz) and
+// d = (s_hi - t_hi) + (s_lo - t_lo) carries the FP32 relative accuracy of |d| itself
+// (absolute error ~2^-48 of the root box), however small |d| is.  No per-leaf shift
+// is needed, so the sources of many U-list entries are staged together.
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     const float y = v - c;
     const float t = s + y;
@@ -633,103 +635,181 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t;
 }
 
-constexpr int NEAR_STAGE = 64;
+constexpr int NEAR_CAP = 128;    // source bodies staged per round (several U-list entries)
+constexpr int NEAR_UNITS = 64;   // (target, source part) units per target chunk: two per lane
 
-// softened pair sum over staged sources q = q0, q0 + dq, ... < n
+__global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restrict__ rhi, float4* __restrict__ rlo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tv.n) return;
+    const double ex = tv.px[i] - tv.root->c[0], ey = tv.py[i] - tv.root->c[1], ez = tv.pz[i] - tv.root->c[2];
+    const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
+    rhi[i] = make_float4(hx, hy, hz, (float)tv.pm[i]);
+    rlo[i] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+}
+
+// softened pair sum of one target over staged sources q = q0, q0 + dq, ... < n;
+// SELF: the source at staged position self_q is the target itself and is skipped
 template <bool SELF, bool POT>
-__device__ __forceinline__ void p2p_block(const float4* __restrict__ shi, const float4* __restrict__ slo, int q0, int dq, int n,
-                                          int self_q, float thx, float thy, float thz, float tlx, float tly, float tlz,
-                                          float eps2, float& ax, float& ay, float& az, float& ph) {
+__device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const float4* __restrict__ slo, int q0, int dq, int n,
+                                         int self_q, const float (&th)[3], const float (&tl)[3], float eps2, float (&a)[4]) {
 #pragma unroll 4
     for (int q = q0; q < n; q += dq) {
         const float4 h = shi[q];
         const float4 l = slo[q];
-        const float dx = (h.x - thx) + (l.x - tlx);
-        const float dy = (h.y - thy) + (l.y - tly);
-        const float dz = (h.z - thz) + (l.z - tlz);
+        const float dx = (h.x - th[0]) + (l.x - tl[0]);
+        const float dy = (h.y - th[1]) + (l.y - tl[1]);
+        const float dz = (h.z - th[2]) + (l.z - tl[2]);
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
         const bool self = SELF && (q == self_q);
-        const float r2s = self ? 1.0f : r2;
         // rsqrtf alone (within 2 ulp): its error, ~1e-7 per pair in random directions,
-        // stays far below the form's budget, and a Newton step would cost 3 of the
-        // pair's ~24 instructions
-        const float y = rsqrtf(r2s);
-        const float m = self ? 0.0f : h.w;
-        const float my = m * y;
+        // stays far below the form's budget
+        const float y = rsqrtf(self ? 1.0f : r2);
+        const float my = (self ? 0.0f : h.w) * y;
         const float w = my * y * y;
-        ax = fmaf(w, dx, ax);
-        ay = fmaf(w, dy, ay);
-        az = fmaf(w, dz, az);
-        if (POT) ph += my;
+        a[0] = fmaf(w, dx, a[0]);
+        a[1] = fmaf(w, dy, a[1]);
+        a[2] = fmaf(w, dz, a[2]);
+        if (POT) a[3] += my;
     }
 }
 
-__device__ __forceinline__ double group_sum(double v, int tpg) {
-    for (int off = tpg; off < 32; off <<= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    return v;
+// Number of source parts G for a chunk of T targets: units (target, part) = T G are
+// spread over the 32 lanes in R = ceil(T G / 32) <= 2 rounds; G maximises the busy
+// fraction T G / (32 R) (ties: the smaller G).  A 17-body leaf gets G = 3 (80% busy;
+// one target per lane would leave 47% of the lanes idle), a 5-body leaf G = 6 (94%).
+__device__ __forceinline__ int near_parts(int T) {
+    int best = 1, bu = 0;
+    for (int G = 1; G <= 32 && T * G <= NEAR_UNITS; ++G) {
+        const int U = T * G;
+        const int u = (U << 10) / (32 * ((U + 31) >> 5));   // busy fraction, fixed point
+        if (u > bu) { bu = u; best = G; }
+    }
+    return best;
 }
 
-// Warp per leaf (one warp per block, so a block's resources return as soon as
-// its leaf is done).  A leaf of cnt <= 32 bodies splits the warp into G groups
-// of tpg = next power of two >= cnt lanes: lane (g, t) owns target body t and
-// takes every G-th source of each staged block, so small leaves keep most lanes
-// busy; the groups' partial sums (compensated per U entry) are combined in FP64
-// with shuffles.  Larger leaves run 32 targets at a time with G = 1.  Output:
-// near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64; the kernel
-// needs only the tree and lists, so it runs beside the far-field chain.
-// Block b takes leaves b, b + gridDim.x, ... (one leaf per block at the usual
-// grid of one block per leaf).
+// Warp per target leaf (one warp per block, so a block's resources return as soon as
+// its leaf is done).  The leaf's bodies go in chunks of up to 32 targets; in a chunk
+// of T targets, unit u = lane + 32 r (r < 2) is target u mod T with source part
+// u / T, which takes every G-th source of each staged round.  The leaf itself is one
+// round (with the self pair skipped); the bodies of all other U-list entries are
+// concatenated and staged NEAR_CAP at a time.  Each unit folds every round's partial
+// sum into a compensated (Kahan) accumulator; at the end the G parts of each target
+// are added in part order in FP64 through shared memory (deterministic).  Output:
+// near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64.  The kernel needs
+// only the tree and the lists, so it runs beside the far-field chain.
 template <bool POT>
-__global__ void __launch_bounds__(32) k_leaf_near32(TreeView tv, float eps2, double* __restrict__ near) {
-    __shared__ float4 s_hi[NEAR_STAGE], s_lo[NEAR_STAGE];
+__global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float4* __restrict__ rhi,
+                                                        const float4* __restrict__ rlo, float eps2, double* __restrict__ near) {
+    __shared__ float4 s_hi[NEAR_CAP], s_lo[NEAR_CAP];
+    __shared__ double s_red[NEAR_UNITS][4];
     const int lane = threadIdx.x & 31;
     for (int lf = blockIdx.x; lf < tv.nleaf; lf += gridDim.x) {
         const int b = tv.leafbox[lf];
         const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-        const double bcx = tv.center[4 * b], bcy = tv.center[4 * b + 1], bcz = tv.center[4 * b + 2];
         const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
-        int tpg = 1;
-        while (tpg < min(cnt, 32)) tpg <<= 1;
-        const int ngrp = 32 / tpg, grp = lane / tpg, tl = lane & (tpg - 1);
-        for (int j0 = 0; j0 < cnt; j0 += tpg) {
-            const int jj = j0 + tl;
-            const bool act = jj < cnt;
-            const int i = f0 + (act ? jj : 0);
-            const double ddx = tv.px[i] - bcx, ddy = tv.py[i] - bcy, ddz = tv.pz[i] - bcz;
-            const float thx = (float)ddx, thy = (float)ddy, thz = (float)ddz;
-            const float tlx = (float)(ddx - (double)thx), tly = (float)(ddy - (double)thy), tlz = (float)(ddz - (double)thz);
-            float sx = 0, sy = 0, sz = 0, sp = 0, cx = 0, cy = 0, cz = 0, cp = 0;
-            for (int64_t e = u0; e < u1; ++e) {
-                const int c = tv.u_idx[e];
-                const int s0 = tv.pfirst[c], sc = tv.pcount[c];
-                float ax = 0, ay = 0, az = 0, ph = 0;
-                for (int k0 = 0; k0 < sc; k0 += NEAR_STAGE) {
-                    const int n = min(NEAR_STAGE, sc - k0);
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            const int T = min(32, cnt - j0);
+            const int G = near_parts(T);
+            const int U = T * G;
+            // the lane's two units: target tt[r] (index in the leaf), source part pp[r]
+            int tt[2], pp[2];
+            bool act[2];
+            float th[2][3], tl[2][3];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int u = lane + 32 * r;
+                act[r] = u < U;
+                tt[r] = act[r] ? u % T : 0;
+                pp[r] = act[r] ? u / T : 0;
+                const float4 h = rhi[f0 + j0 + tt[r]], l = rlo[f0 + j0 + tt[r]];
+                th[r][0] = h.x; th[r][1] = h.y; th[r][2] = h.z;
+                tl[r][0] = l.x; tl[r][1] = l.y; tl[r][2] = l.z;
+            }
+            float ks[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            float kc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            // round 0: the leaf itself
+            for (int k0 = 0; k0 < cnt; k0 += NEAR_CAP) {
+                const int n = min(NEAR_CAP, cnt - k0);
+                __syncwarp();
+                for (int q = lane; q < n; q += 32) {
+                    s_hi[q] = rhi[f0 + k0 + q];
+                    s_lo[q] = rlo[f0 + k0 + q];
+                }
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                    if (!act[r]) continue;
+                    float a[4] = {0.f, 0.f, 0.f, 0.f};
+                    p2p_part<true, POT>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);
+                }
+            }
+            // the other U-list entries, 32 at a time: lane e holds entry e's first body and
+            // count; an inclusive scan of the counts maps a flat source position to its entry
+            for (int64_t eb = u0; eb < u1; eb += 32) {
+                const int64_t e = eb + lane;
+                int pf = 0, pc = 0;
+                if (e < u1) {
+                    const int c = tv.u_idx[e];
+                    if (c != b) { pf = tv.pfirst[c]; pc = tv.pcount[c]; }
+                }
+                int pre = pc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, pre, o);
+                    if (lane >= o) pre += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, pre, 31);
+                for (int base = 0; base < total; base += NEAR_CAP) {
+                    const int n = min(NEAR_CAP, total - base);
                     __syncwarp();
-                    for (int q = lane; q < n; q += 32) {
-                        const int j = s0 + k0 + q;
-                        const double ex = tv.px[j] - bcx, ey = tv.py[j] - bcy, ez = tv.pz[j] - bcz;
-                        const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
-                        s_hi[q] = make_float4(hx, hy, hz, (float)tv.pm[j]);
-                        s_lo[q] = make_float4((float)(ex - (double)hx), (float)(ey - (double)hy), (float)(ez - (double)hz), 0.f);
+                    // warp-uniform trip count: every lane takes part in every shuffle
+                    for (int q0 = 0; q0 < n; q0 += 32) {
+                        const int q = q0 + lane;
+                        const int f = base + q;
+                        // entry of flat position f: the number of entries whose inclusive
+                        // prefix is <= f (five halving steps over the 32 prefixes)
+                        int pos = 0;
+#pragma unroll
+                        for (int step = 16; step > 0; step >>= 1)
+                            if (__shfl_sync(0xffffffffu, pre, pos + step - 1) <= f) pos += step;
+                        const int ep = __shfl_sync(0xffffffffu, pre, pos), ec = __shfl_sync(0xffffffffu, pc, pos);
+                        const int j = __shfl_sync(0xffffffffu, pf, pos) + f - (ep - ec);
+                        if (q < n) {
+                            s_hi[q] = rhi[j];
+                            s_lo[q] = rlo[j];
+                        }
                     }
                     __syncwarp();
-                    if (c == b)
-                        p2p_block<true, POT>(s_hi, s_lo, grp, ngrp, n, i - s0 - k0, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
-                    else
-                        p2p_block<false, POT>(s_hi, s_lo, grp, ngrp, n, -1, thx, thy, thz, tlx, tly, tlz, eps2, ax, ay, az, ph);
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        if (!act[r]) continue;
+                        float a[4] = {0.f, 0.f, 0.f, 0.f};
+                        p2p_part<false, POT>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);
+                    }
                 }
-                kahan_add(sx, cx, ax); kahan_add(sy, cy, ay); kahan_add(sz, cz, az);
-                if (POT) kahan_add(sp, cp, ph);
             }
-            const double nx = group_sum((double)sx - (double)cx, tpg);
-            const double ny = group_sum((double)sy - (double)cy, tpg);
-            const double nz = group_sum((double)sz - (double)cz, tpg);
-            const double np = POT ? group_sum((double)sp - (double)cp, tpg) : 0.0;
-            if (act && grp == 0) {
-                double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)i);
-                o[0] = make_double2(nx, ny);
-                o[1] = make_double2(nz, np);
+            // the parts of every target, in part order, in FP64
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                if (act[r])
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) s_red[lane + 32 * r][k] = (double)ks[r][k] - (double)kc[r][k];
+            __syncwarp();
+            if (lane < T) {
+                double v[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int p = 0; p < G; ++p)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) v[k] += s_red[p * T + lane][k];
+                double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)(f0 + j0 + lane));
+                o[0] = make_double2(v[0], v[1]);
+                o[1] = make_double2(v[2], POT ? v[3] : 0.0);
             }
         }
         __syncwarp();
