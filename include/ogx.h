@@ -122,6 +122,24 @@ int ogx_direct_eval_noalloc(int64_t n, const double* pos, const double* mass, do
 const char* ogx_name(void* handle);
 int ogx_last_stats(void* handle, ogx_stats* out);
 const char* ogx_strerror(int status);
+/* Launch-shape knobs of the mixed form (no counterpart in the reference, whose only knob is
+ * the leaf capacity, AdaptiveFMM3D(KernelParams3D, int p, int threshold),
+ * src3d/AdaptiveFMM3D.hpp:22-23).  Neither changes what is computed:
+ *   m2l_tile_targets : M2L batch width, the targets placed in one 128-row tensor-core tile
+ *                      (32, 64, 96 or 128; default 128).  Narrower batches give small
+ *                      systems more tiles to spread over the SMs.  A target's M2L result
+ *                      does not depend on it.
+ *   near_units       : P2P tile shape, the (target, source part) units a warp spreads over
+ *                      its 32 lanes per chunk of up to 32 targets (32 or 64; default 64).
+ *                      64 lets a small leaf split its sources into more parts; it changes
+ *                      the FP32 summation order of the near field only.
+ * ogx_set_tuning applies from the next evaluation on; 0 in a field keeps its default. */
+typedef struct {
+    int m2l_tile_targets;
+    int near_units;
+} ogx_tuning;
+int ogx_set_tuning(void* handle, const ogx_tuning* t);
+int ogx_get_tuning(void* handle, ogx_tuning* out);
 /* Diagnostic with no counterpart in the reference: runs the bounded device wait of the
  * tensor-core M2L pipeline (an mbarrier wait that gives up after a poll limit and sets the
  * handle's device error word) on a barrier that nothing arrives on, with `polls` (>= 1) as the

@@ -16,9 +16,17 @@
 // --ensemble --steps S: the batched-ensemble workload instead.  All systems are
 // resident together and advance in lockstep (every system finishes step s before any
 // starts step s + 1), their steps spread over the same worker pool; the line then also
-// carries the lockstep step time (p50 / p99).  --autotune picks each system's leaf
-// capacity from {32, 48, 64, 96, 128} by timing force evaluations of that system alone
-// before the run; --thr fixes it instead (default 64).
+// carries the lockstep step time (p50 / p99).
+//
+// --autotune picks three knobs per job before it runs, by timing steps of dt = 0 of
+// that job alone (a coordinate search): the leaf capacity from {32, 48, 64, 96, 128}
+// (--thr fixes it instead, default 64), then the M2L batch width (targets per
+// tensor-core tile) from {32, 64, 96, 128}, then the P2P tile shape (near-field units
+// per warp) from {32, 64}.  The two launch-shape knobs change no physics: a candidate
+// is only accepted when its accelerations agree with those of the default shape to a
+// relative RMS of 1e-6.  --tune-cache FILE keeps the choices per (initial-condition
+// kind, N rounded to a power of two, p, precision) as JSON: read before the run, the
+// entries found skip the search, and the file is rewritten with every choice after it.
 //
 // Prints one JSON line: per-step latency p50 / p99 (the time from a step call until its
 // result is on the device, ogx_step + ogx_synchronize), job turnaround p50 / p99 (from
@@ -35,6 +43,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <random>
 #include <string>
@@ -55,6 +64,9 @@ struct Job {
     int steps = 10;
     int kind = 0;  // 0 Plummer, 1 two-galaxy disk+bulge
     int thr = 64;  // leaf capacity
+    int fill = 128;   // M2L batch width (targets per tensor-core tile)
+    int units = 64;   // near-field units per warp
+    bool tuned_from_cache = false;
     uint64_t seed = 0;
     // results
     uint64_t digest = 0;
@@ -135,6 +147,11 @@ void* open_job(Job& job, int precision) {
     prm.precision = precision;
     void* h = nullptr;
     if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return nullptr;
+    ogx_tuning tu{job.fill, job.units};
+    if ((job.status = ogx_set_tuning(h, &tu)) != OGX_OK) {
+        ogx_destroy(h);
+        return nullptr;
+    }
     if (job.kind == 0) {
         std::vector<double> pos, vel, mass;
         plummer(job.n, job.seed, pos, vel, mass);
@@ -177,31 +194,131 @@ void run_job(Job& job, int precision) {
     close_job(job, h);
 }
 
-// leaf capacity of a job from a short trial: the candidate whose second force
-// evaluation (a step of dt = 0 leaves the state unchanged) is fastest when run alone
-int autotune_thr(Job job, int precision) {
-    static const int cands[] = {32, 48, 64, 96, 128};
-    int best = job.thr;
+// fastest of the second and third of three steps of dt = 0 (the state is unchanged)
+float time_steps(Job& job, void* h) {
+    float ms = 1e30f;
+    for (int r = 0; r < 3 && job.status == OGX_OK; ++r) {
+        const auto t0 = std::chrono::steady_clock::now();
+        job.status = ogx_step(h, 0.0, 1);
+        if (job.status == OGX_OK) job.status = ogx_synchronize(h);
+        if (r > 0) ms = std::min(ms, (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+    return job.status == OGX_OK ? ms : 1e30f;
+}
+
+double rms_rel(const std::vector<double>& ref, const std::vector<double>& got) {
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < ref.size(); ++i) {
+        num += (got[i] - ref[i]) * (got[i] - ref[i]);
+        den += ref[i] * ref[i];
+    }
+    return den > 0.0 ? std::sqrt(num / den) : 0.0;
+}
+
+struct TuneChoice {
+    int thr = 64, fill = 128, units = 64;
+    float ms = 0.f;
+};
+
+// the knobs of one job, by coordinate search (see the file comment)
+TuneChoice tune_job(Job job, int precision) {
+    static const int thrs[] = {32, 48, 64, 96, 128};
+    static const int fills[] = {32, 64, 96, 128};
+    static const int unitss[] = {32, 64};
+    TuneChoice best;
+    best.thr = job.thr;
     float best_ms = 1e30f;
-    for (int thr : cands) {
+    job.fill = 128;
+    job.units = 64;
+    for (int thr : thrs) {
         job.thr = thr;
-        job.step_ms.clear();
+        job.status = OGX_OK;
         void* h = open_job(job, precision);
         if (!h) continue;
-        float ms = 1e30f;
-        for (int r = 0; r < 3 && job.status == OGX_OK; ++r) {
-            const auto t0 = std::chrono::steady_clock::now();
-            job.status = ogx_step(h, 0.0, 1);
-            if (job.status == OGX_OK) job.status = ogx_synchronize(h);
-            if (r > 0) ms = std::min(ms, (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-        }
+        const float ms = time_steps(job, h);
         ogx_destroy(h);
-        if (job.status == OGX_OK && ms < best_ms) {
+        if (ms < best_ms) {
             best_ms = ms;
-            best = thr;
+            best.thr = thr;
         }
     }
+    best.ms = best_ms;
+    if (precision != OGX_PREC_MIXED) return best;   // the launch-shape knobs serve the mixed form
+    job.thr = best.thr;
+    job.status = OGX_OK;
+    void* h = open_job(job, precision);
+    if (!h) return best;
+    const int64_t n = (job.kind == 0) ? job.n : 2 * (job.n / 2);
+    std::vector<double> ref(3 * n), acc(3 * n);
+    // accelerations of the default shape, then each candidate shape on the same state
+    if (ogx_step(h, 0.0, 1) != OGX_OK || ogx_download(h, nullptr, nullptr, ref.data()) != OGX_OK) {
+        ogx_destroy(h);
+        return best;
+    }
+    auto trial = [&](int fill, int units) -> float {
+        ogx_tuning tu{fill, units};
+        if (ogx_set_tuning(h, &tu) != OGX_OK) return 1e30f;
+        const float ms = time_steps(job, h);
+        if (ms >= 1e30f || ogx_download(h, nullptr, nullptr, acc.data()) != OGX_OK) return 1e30f;
+        return rms_rel(ref, acc) <= 1e-6 ? ms : 1e30f;   // accuracy gate
+    };
+    float cur = trial(128, 64);
+    for (int fill : fills) {
+        if (fill == 128) continue;
+        const float ms = trial(fill, best.units);
+        if (ms < cur) {
+            cur = ms;
+            best.fill = fill;
+        }
+    }
+    for (int units : unitss) {
+        if (units == best.units) continue;
+        const float ms = trial(best.fill, units);
+        if (ms < cur) {
+            cur = ms;
+            best.units = units;
+        }
+    }
+    best.ms = std::min(best_ms, cur);
+    ogx_destroy(h);
     return best;
+}
+
+// --tune-cache: {"<kind>:n<log2 N>:p<p>:<precision>": {"leaf_capacity": .., "m2l_tile_targets": ..,
+// "near_units": .., "ms": ..}, ...}, one entry per line (this program writes and reads it)
+std::string tune_key(const Job& jb, int precision) {
+    const int lg = (int)std::lround(std::log2((double)std::max<int64_t>(jb.n, 1)));
+    return std::string(jb.kind ? "merger" : "plummer") + ":n" + std::to_string(lg) + ":p" + std::to_string(jb.p) + ":" +
+           (precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed");
+}
+
+std::map<std::string, TuneChoice> read_tune_cache(const std::string& path) {
+    std::map<std::string, TuneChoice> m;
+    FILE* f = path.empty() ? nullptr : std::fopen(path.c_str(), "r");
+    if (!f) return m;
+    char line[512];
+    while (std::fgets(line, sizeof line, f)) {
+        char key[256];
+        TuneChoice c;
+        if (std::sscanf(line, " \"%255[^\"]\": {\"leaf_capacity\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, \"ms\": %f",
+                        key, &c.thr, &c.fill, &c.units, &c.ms) == 5)
+            m[key] = c;
+    }
+    std::fclose(f);
+    return m;
+}
+
+void write_tune_cache(const std::string& path, const std::map<std::string, TuneChoice>& m) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return;
+    std::fprintf(f, "{\n");
+    size_t k = 0;
+    for (const auto& kv : m)
+        std::fprintf(f, "\"%s\": {\"leaf_capacity\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, \"ms\": %.4f}%s\n",
+                     kv.first.c_str(), kv.second.thr, kv.second.fill, kv.second.units, kv.second.ms,
+                     ++k < m.size() ? "," : "");
+    std::fprintf(f, "}\n");
+    std::fclose(f);
 }
 
 // samples the device's used memory every millisecond while armed (solo runs)
@@ -252,6 +369,7 @@ int main(int argc, char** argv) {
     int64_t nmin = 16384, nmax = 1 << 20;
     uint64_t seed = 1;
     bool solo = false, ensemble = false, autotune = false;
+    std::string tune_cache;
     int precision = OGX_PREC_MIXED, thr = 64, workers = 8;
     std::vector<int> orders = {6, 8, 12};
     for (int i = 1; i < argc; ++i) {
@@ -268,6 +386,7 @@ int main(int argc, char** argv) {
         else if (a == "--solo") solo = true;
         else if (a == "--ensemble") ensemble = true;
         else if (a == "--autotune") autotune = true;
+        else if (a == "--tune-cache") tune_cache = next();
         else if (a == "--thr") thr = std::atoi(next().c_str());
         else if (a == "--workers") workers = std::atoi(next().c_str());
         else if (a == "--steps") smin = smax = std::atoi(next().c_str());
@@ -303,6 +422,7 @@ int main(int argc, char** argv) {
     // the seeded job stream
     std::mt19937_64 rng(seed);
     auto uni = [&]() { return (double)(rng() >> 11) * (1.0 / 9007199254740992.0); };
+    std::map<std::string, TuneChoice> tcache = read_tune_cache(tune_cache);
     std::vector<Job> jobs(njobs);
     double t = 0.0;
     for (int j = 0; j < njobs; ++j) {
@@ -448,7 +568,15 @@ int main(int argc, char** argv) {
                 continue;
             }
             in_use += jb.need_bytes;
-            if (autotune) jb.thr = autotune_thr(jb, precision);
+            if (autotune) {
+                const std::string key = tune_key(jb, precision);
+                auto it = tcache.find(key);
+                if (it == tcache.end()) it = tcache.emplace(key, tune_job(jb, precision)).first;
+                else jb.tuned_from_cache = true;
+                jb.thr = it->second.thr;
+                jb.fill = it->second.fill;
+                jb.units = it->second.units;
+            }
             live.push_back(&jb);
         }
         const int L = (int)live.size();
@@ -500,13 +628,16 @@ int main(int argc, char** argv) {
                     percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s);
         for (size_t j = 0; j < jobs.size(); ++j) {
             const Job& jb = jobs[j];
-            std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"kind\": \"%s\", \"status\": %d, "
+            std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, "
+                        "\"tuned_from_cache\": %s, \"kind\": \"%s\", \"status\": %d, "
                         "\"rejected\": %s, \"step_ms_p50\": %.3f, \"digest\": \"%016llx\"}",
-                        j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.kind ? "disk+bulge merger" : "plummer",
+                        j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.fill, jb.units,
+                        jb.tuned_from_cache ? "true" : "false", jb.kind ? "disk+bulge merger" : "plummer",
                         jb.status, jb.rejected ? "true" : "false", percentile(jb.step_ms, 0.5),
                         (unsigned long long)jb.digest);
         }
         std::printf("]}\n");
+        if (autotune && !tune_cache.empty()) write_tune_cache(tune_cache, tcache);
         return failed ? 1 : 0;
     }
 
@@ -521,7 +652,15 @@ int main(int argc, char** argv) {
             ++rejected;
             continue;
         }
-        if (autotune) jb.thr = autotune_thr(jb, precision);
+        if (autotune) {
+            const std::string key = tune_key(jb, precision);
+            auto it = tcache.find(key);
+            if (it == tcache.end()) it = tcache.emplace(key, tune_job(jb, precision)).first;
+            else jb.tuned_from_cache = true;
+            jb.thr = it->second.thr;
+            jb.fill = it->second.fill;
+            jb.units = it->second.units;
+        }
         if (solo) {
             sampler.peak = 0.0;
             sampler.armed = true;
@@ -578,14 +717,17 @@ int main(int argc, char** argv) {
                 solo ? "null" : std::to_string(percentile(turnaround, 0.99)).c_str(), solo ? 1 : peak, hbm_gb);
     for (size_t j = 0; j < jobs.size(); ++j) {
         const Job& jb = jobs[j];
-        std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"steps\": %d, \"kind\": \"%s\", "
+        std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, "
+                    "\"tuned_from_cache\": %s, \"steps\": %d, \"kind\": \"%s\", "
                     "\"status\": %d, \"rejected\": %s, \"need_mb\": %.1f, \"peak_mb\": %.1f, \"step_ms_p50\": %.3f, "
                     "\"digest\": \"%016llx\"}",
-                    j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.steps,
+                    j ? ", " : "", jb.id, (long long)jb.n, jb.p, jb.thr, jb.fill, jb.units,
+                    jb.tuned_from_cache ? "true" : "false", jb.steps,
                     jb.kind ? "disk+bulge merger" : "plummer", jb.status, jb.rejected ? "true" : "false",
                     jb.need_bytes / 1e6, jb.peak_bytes / 1e6, percentile(jb.step_ms, 0.5),
                     (unsigned long long)jb.digest);
     }
     std::printf("]}\n");
+    if (autotune && !tune_cache.empty()) write_tune_cache(tune_cache, tcache);
     return failed ? 1 : 0;
 }

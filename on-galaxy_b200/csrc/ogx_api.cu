@@ -619,6 +619,28 @@ int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx) {
     return OGX_OK;
 }
 
+int ogx_set_tuning(void* handle, const ogx_tuning* t) {
+    if (!handle || !t) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    const int fill = t->m2l_tile_targets ? t->m2l_tile_targets : 128;
+    const int units = t->near_units ? t->near_units : 64;
+    if ((fill != 32 && fill != 64 && fill != 96 && fill != 128) || (units != 32 && units != 64)) {
+        set_last_error(OGX_ERR_INVALID, "ogx_set_tuning: m2l_tile_targets must be 32, 64, 96 or 128 and near_units 32 or 64");
+        return OGX_ERR_INVALID;
+    }
+    h.tile_fill = fill;
+    h.near_units = units;
+    return OGX_OK;
+}
+
+int ogx_get_tuning(void* handle, ogx_tuning* out) {
+    if (!handle || !out) return OGX_ERR_INVALID;
+    HANDLE(handle);
+    out->m2l_tile_targets = h.tile_fill;
+    out->near_units = h.near_units;
+    return OGX_OK;
+}
+
 int ogx_check_bounded_wait(void* handle, uint32_t polls) {
     if (!handle || polls == 0) return OGX_ERR_INVALID;
     HANDLE(handle);

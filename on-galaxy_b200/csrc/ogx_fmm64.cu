@@ -562,8 +562,9 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
         mixed::k_near_prep<<<(tv.n + 255) / 256, 256, 0, h.side>>>(tv, rel, rel + tv.n); ++h.launches;
         const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
-        if (d_pot) { mixed::k_leaf_near32<true><<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches; }
-        else { mixed::k_leaf_near32<false><<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches; }
+        auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32> : mixed::k_leaf_near32<true, 64>)
+                          : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32> : mixed::k_leaf_near32<false, 64>);
+        near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches;
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
     OGX_CUDA(cudaEventRecord(h.ev[4], st));

@@ -220,6 +220,9 @@ struct Handle {
     float* d_tc_ounscale = nullptr; // per M2L operator: 2^e undoing the scaling of its FP16 images
     int* d_err = nullptr;          // device error word of the bounded waits
     int* h_err = nullptr;          // pinned copy
+    // launch-shape knobs (ogx_set_tuning)
+    int tile_fill = 128;    // targets per 128-row M2L tile
+    int near_units = 64;    // (target, source part) units per near-field chunk
     // M2L targets (levels >= 2) sorted by child octant
     int ntgt = 0;
     const uint32_t* tgt_key = nullptr;

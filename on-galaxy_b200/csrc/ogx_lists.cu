@@ -277,7 +277,7 @@ __global__ void k_tgt_keys(int first, int nb, const int* __restrict__ coord, con
 // bits 27-29): every octant group starts on a multiple of `tile`, so a tile never
 // mixes octants.  gs[0..8] = group starts,
 // gs[9..17] = padded group starts.
-__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int* gs) {
+__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int fill, int* gs) {
     __shared__ int lo_s[9];
     const int g = threadIdx.x;
     if (g <= 8) {
@@ -294,19 +294,23 @@ __global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int* gs
         int pad = 0;
         for (int q = 0; q <= 8; ++q) {
             gs[9 + q] = pad;
-            if (q < 8) pad += ((lo_s[q + 1] - lo_s[q] + tile - 1) / tile) * tile;
+            if (q < 8) pad += ((lo_s[q + 1] - lo_s[q] + fill - 1) / fill) * tile;
         }
     }
 }
-__global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, uint32_t* pkey, uint32_t* pbox) {
+// slot q of a padded group holds target (q - start) / tile * fill + (q - start) % tile
+// when that slot index is below `fill` (the batch width) and the target exists
+__global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, int tile, int fill, uint32_t* pkey,
+                             uint32_t* pbox) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npad) return;
     uint32_t k = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
     for (int g = 0; g < 8; ++g) {
         const int ps = gs[9 + g], pe = gs[9 + g + 1];
         if (q >= ps && q < pe) {
-            const int local = q - ps;
-            if (local < gs[g + 1] - gs[g]) { k = (uint32_t)g; b = box[gs[g] + local]; }
+            const int slot = (q - ps) % tile;
+            const int local = (q - ps) / tile * fill + slot;
+            if (slot < fill && local < gs[g + 1] - gs[g]) { k = (uint32_t)g; b = box[gs[g] + local]; }
             break;
         }
     }
@@ -395,14 +399,15 @@ int lists_build(Handle& h) {
         h.tgt_key = tk_s;
         h.tgt_box = tb_s;
         const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
-        const int npad = ((ntgt + tile - 1) / tile + 8) * tile;
+        const int fill = h.tile_fill;   // targets per tile (the M2L batch width)
+        const int npad = ((ntgt + fill - 1) / fill + 8) * tile;
         int* gs;
         uint32_t *pk, *pb;
         OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
         OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
         OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
-        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, gs); ++h.launches;
-        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, pk, pb); ++h.launches;
+        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, fill, gs); ++h.launches;
+        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, tile, fill, pk, pb); ++h.launches;
         h.tgt_tile_key = pk;
         h.tgt_tile_box = pb;
         h.ntgt_pad = npad;

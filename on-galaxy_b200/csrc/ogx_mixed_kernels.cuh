@@ -636,7 +636,6 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 }
 
 constexpr int NEAR_CAP = 128;    // source bodies staged per round (several U-list entries)
-constexpr int NEAR_UNITS = 64;   // (target, source part) units per target chunk: two per lane
 
 __global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restrict__ rhi, float4* __restrict__ rlo) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -673,13 +672,15 @@ __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const f
     }
 }
 
-// Number of source parts G for a chunk of T targets: units (target, part) = T G are
-// spread over the 32 lanes in R = ceil(T G / 32) <= 2 rounds; G maximises the busy
-// fraction T G / (32 R) (ties: the smaller G).  A 17-body leaf gets G = 3 (80% busy;
-// one target per lane would leave 47% of the lanes idle), a 5-body leaf G = 6 (94%).
+// Number of source parts G for a chunk of T targets: units (target, part) = T G,
+// at most NU, are spread over the 32 lanes in R = ceil(T G / 32) rounds; G maximises
+// the busy fraction T G / (32 R) (ties: the smaller G).  With NU = 64 a 17-body leaf
+// gets G = 3 (80% busy; one target per lane would leave 47% of the lanes idle), a
+// 5-body leaf G = 6 (94%).
+template <int NU>
 __device__ __forceinline__ int near_parts(int T) {
     int best = 1, bu = 0;
-    for (int G = 1; G <= 32 && T * G <= NEAR_UNITS; ++G) {
+    for (int G = 1; G <= 32 && T * G <= NU; ++G) {
         const int U = T * G;
         const int u = (U << 10) / (32 * ((U + 31) >> 5));   // busy fraction, fixed point
         if (u > bu) { bu = u; best = G; }
@@ -689,7 +690,7 @@ __device__ __forceinline__ int near_parts(int T) {
 
 // Warp per target leaf (one warp per block, so a block's resources return as soon as
 // its leaf is done).  The leaf's bodies go in chunks of up to 32 targets; in a chunk
-// of T targets, unit u = lane + 32 r (r < 2) is target u mod T with source part
+// of T targets, unit u = lane + 32 r (r < NU / 32) is target u mod T with source part
 // u / T, which takes every G-th source of each staged round.  The leaf itself is one
 // round (with the self pair skipped); the bodies of all other U-list entries are
 // concatenated and staged NEAR_CAP at a time.  Each unit folds every round's partial
@@ -697,11 +698,13 @@ __device__ __forceinline__ int near_parts(int T) {
 // are added in part order in FP64 through shared memory (deterministic).  Output:
 // near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64.  The kernel needs
 // only the tree and the lists, so it runs beside the far-field chain.
-template <bool POT>
+template <bool POT, int NU>
 __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float4* __restrict__ rhi,
                                                         const float4* __restrict__ rlo, float eps2, double* __restrict__ near) {
+    constexpr int R = NU / 32;
+    static_assert(R * 32 == NU && R >= 1 && R <= 2, "near-field units: 32 or 64");
     __shared__ float4 s_hi[NEAR_CAP], s_lo[NEAR_CAP];
-    __shared__ double s_red[NEAR_UNITS][4];
+    __shared__ double s_red[NU][4];
     const int lane = threadIdx.x & 31;
     for (int lf = blockIdx.x; lf < tv.nleaf; lf += gridDim.x) {
         const int b = tv.leafbox[lf];
@@ -709,14 +712,14 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
         const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
         for (int j0 = 0; j0 < cnt; j0 += 32) {
             const int T = min(32, cnt - j0);
-            const int G = near_parts(T);
+            const int G = near_parts<NU>(T);
             const int U = T * G;
-            // the lane's two units: target tt[r] (index in the leaf), source part pp[r]
-            int tt[2], pp[2];
-            bool act[2];
-            float th[2][3], tl[2][3];
+            // the lane's units: target tt[r] (index in the leaf), source part pp[r]
+            int tt[R], pp[R];
+            bool act[R];
+            float th[R][3], tl[R][3];
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
+            for (int r = 0; r < R; ++r) {
                 const int u = lane + 32 * r;
                 act[r] = u < U;
                 tt[r] = act[r] ? u % T : 0;
@@ -725,8 +728,11 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                 th[r][0] = h.x; th[r][1] = h.y; th[r][2] = h.z;
                 tl[r][0] = l.x; tl[r][1] = l.y; tl[r][2] = l.z;
             }
-            float ks[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-            float kc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+            float ks[R][4], kc[R][4];
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ks[r][k] = kc[r][k] = 0.f;
             // round 0: the leaf itself
             for (int k0 = 0; k0 < cnt; k0 += NEAR_CAP) {
                 const int n = min(NEAR_CAP, cnt - k0);
@@ -737,7 +743,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                 }
                 __syncwarp();
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < R; ++r) {
                     if (!act[r]) continue;
                     float a[4] = {0.f, 0.f, 0.f, 0.f};
                     p2p_part<true, POT>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a);
@@ -784,7 +790,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                     }
                     __syncwarp();
 #pragma unroll
-                    for (int r = 0; r < 2; ++r) {
+                    for (int r = 0; r < R; ++r) {
                         if (!act[r]) continue;
                         float a[4] = {0.f, 0.f, 0.f, 0.f};
                         p2p_part<false, POT>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a);
@@ -797,7 +803,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
             // the parts of every target, in part order, in FP64
             __syncwarp();
 #pragma unroll
-            for (int r = 0; r < 2; ++r)
+            for (int r = 0; r < R; ++r)
                 if (act[r])
 #pragma unroll
                     for (int k = 0; k < 4; ++k) s_red[lane + 32 * r][k] = (double)ks[r][k] - (double)kc[r][k];

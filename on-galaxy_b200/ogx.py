@@ -32,7 +32,7 @@ EXPORTS = (
     "ogx_name", "ogx_last_stats", "ogx_strerror", "ogx_last_error_message", "ogx_operator_matrix",
     "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
     "ogx_direct_eval_noalloc", "ogx_merger_params_default", "ogx_ic_merger", "ogx_set_species",
-    "ogx_diagnostics", "ogx_download_frame", "ogx_check_bounded_wait",
+    "ogx_diagnostics", "ogx_download_frame", "ogx_check_bounded_wait", "ogx_set_tuning", "ogx_get_tuning",
 )
 
 
@@ -53,6 +53,10 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [("m2l_tile_targets", C.c_int), ("near_units", C.c_int)]
 
 
 class MergerParams(C.Structure):
@@ -113,6 +117,8 @@ def load(path: str = LIB_PATH):
     lib.ogx_diagnostics.argtypes = [vp, dp]
     lib.ogx_download_frame.argtypes = [vp, vp]
     lib.ogx_check_bounded_wait.argtypes = [vp, C.c_uint32]
+    lib.ogx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+    lib.ogx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
     _lib = lib
     return lib
 
@@ -213,6 +219,16 @@ class _Solver:
 
     def synchronize(self):
         _check(self._lib.ogx_synchronize(self._h), "ogx_synchronize")
+
+    def set_tuning(self, m2l_tile_targets=0, near_units=0):
+        """Launch-shape knobs of the mixed form (0 keeps the default); see ogx_set_tuning."""
+        t = Tuning(int(m2l_tile_targets), int(near_units))
+        _check(self._lib.ogx_set_tuning(self._h, C.byref(t)), "ogx_set_tuning")
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(self._lib.ogx_get_tuning(self._h, C.byref(t)), "ogx_get_tuning")
+        return {"m2l_tile_targets": t.m2l_tile_targets, "near_units": t.near_units}
 
     def check_bounded_wait(self, polls=1000):
         """Run the pipeline's bounded device wait on a barrier nothing arrives on; raises

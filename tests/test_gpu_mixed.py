@@ -81,3 +81,27 @@ def test_bounded_wait_runs_out_and_the_handle_stays_usable(ogx, golden):
             s.synchronize()   # the error word was cleared when it was reported
         a2 = s.compute_accelerations(d["pos"], d["mass"])
     np.testing.assert_array_equal(a1, a2)
+
+
+@pytest.mark.parametrize("units", [32, 64])
+def test_every_tuning_choice_stays_within_the_mixed_tolerance(ogx, golden, units):
+    """The autotuner's launch-shape knobs: the M2L batch width does not change any bit of the
+    result, and every (batch width, near-field units) choice stays within the mixed form's
+    tolerance of the FP64 form (RMS <= 5e-6, as above)."""
+    d = golden("disk4000")
+    with ogx.AdaptiveFMM3D(p=8, threshold=32, precision=ogx.PREC_FP64) as s64:
+        a64 = s64.compute_accelerations(d["pos"], d["mass"])
+    ref = None
+    with ogx.AdaptiveFMM3D(p=8, threshold=32, precision=ogx.PREC_MIXED) as sm:
+        for fill in (32, 64, 96, 128):
+            sm.set_tuning(m2l_tile_targets=fill, near_units=units)
+            assert sm.tuning() == {"m2l_tile_targets": fill, "near_units": units}
+            am = sm.compute_accelerations(d["pos"], d["mass"])
+            _, rms = rel_err(a64, am)
+            assert rms <= 5e-6, (fill, units, rms)
+            if ref is None:
+                ref = am
+            np.testing.assert_array_equal(am, ref)
+        with pytest.raises(ogx.OgxError) as e:
+            sm.set_tuning(m2l_tile_targets=48)
+        assert e.value.code == ogx.ERR_INVALID

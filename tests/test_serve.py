@@ -110,8 +110,22 @@ def test_ensemble_members_match_their_solo_runs():
 
 
 @pytest.mark.gpu
-def test_ensemble_autotune_picks_a_candidate_leaf_capacity():
-    out = _serve("--ensemble", "--steps", 2, "--jobs", 4, "--nmin", 8192, "--nmax", 65536, "--orders", "6,8",
-                 "--seed", 9, "--autotune")
+def test_ensemble_autotune_picks_candidates_and_reuses_its_cache(tmp_path):
+    """The tuner picks leaf capacity, M2L batch width and P2P tile shape from their candidate
+    sets; its JSON cache is written after the run and, read by a second run, gives the same
+    choices without a new search."""
+    cache = tmp_path / "tune.json"
+    args = ("--ensemble", "--steps", 2, "--jobs", 4, "--nmin", 8192, "--nmax", 65536, "--orders", "6,8",
+            "--seed", 9, "--autotune", "--tune-cache", str(cache))
+    out = _serve(*args)
     assert out["failed"] == 0 and out["autotune"] is True
-    assert all(j["thr"] in (32, 48, 64, 96, 128) for j in out["jobs_detail"])
+    for j in out["jobs_detail"]:
+        assert j["thr"] in (32, 48, 64, 96, 128)
+        assert j["m2l_tile_targets"] in (32, 64, 96, 128)
+        assert j["near_units"] in (32, 64)
+    saved = json.loads(cache.read_text())
+    assert saved and all(set(v) == {"leaf_capacity", "m2l_tile_targets", "near_units", "ms"} for v in saved.values())
+    again = _serve(*args)
+    assert all(j["tuned_from_cache"] for j in again["jobs_detail"])
+    pick = lambda o: [(j["thr"], j["m2l_tile_targets"], j["near_units"]) for j in o["jobs_detail"]]  # noqa: E731
+    assert pick(again) == pick(out)
