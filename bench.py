@@ -96,6 +96,7 @@ def parse():
     ap.add_argument("--n-per", type=int, default=N_PER)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-capture", action="store_true", help="eager steps instead of replaying a captured CUDA graph")
     return ap.parse_args()
 
 
@@ -273,6 +274,9 @@ def main():
         pos, vel, mass, _ = ogx_ic.merger(args.n_per, seed=1, accel_fn=ic_solver.compute_accelerations)
     n = mass.shape[0]
     solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local, stream=stream.cuda_stream)
+    # each timed step replays a CUDA graph captured during the warm-up (no count read-back
+    # in the middle of a step; a step that outgrows its capacities is redone eagerly)
+    solver.set_tuning(capture_steps=0 if args.no_capture else 1)
     solver.upload(pos, vel, mass)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -282,9 +286,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+    for _ in range(args.warmup):
         solver.step(DT, 1)
     torch.cuda.synchronize()
+    graph0 = solver.stats()["graph_steps"]
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     phase = []
@@ -392,6 +397,8 @@ def main():
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
         "e2e": {"value": replica_value(n, world, e2e_mean), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
                 "d2h_bytes_per_step": int(24 * n), "ms_per_step": e2e_mean},
+        "step_capture": {"on": not args.no_capture, "graph_steps_timed": int(st["graph_steps"] - graph0),
+                         "eager_redos": int(st["step_redos"])},
         "phases_ms": phases, "tree": {k: st[k] for k in ("num_boxes", "num_leaves", "max_level", "max_leaf_occupancy",
                                                           "list_u", "list_v", "list_w", "p2p_pairs", "m2p_evals")},
         "pair_interactions_per_s": st["p2p_pairs"] * world / (ms_per_step / 1e3),

@@ -78,6 +78,8 @@ typedef struct {
     double ms_tree, ms_lists, ms_upward, ms_m2l, ms_p2l, ms_downward, ms_leaf, ms_total;
     double ms_h2d, ms_d2h;     /* host-buffer calls only */
     int64_t launches;          /* kernels launched by the last evaluation (+ drift/kick in ogx_step) */
+    int64_t graph_steps;       /* ogx_step calls' steps replayed from a captured graph (running total) */
+    int64_t step_redos;        /* steps redone eagerly after a capacity overflow (running total) */
 } ogx_stats;
 
 /* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0. */
@@ -133,10 +135,20 @@ const char* ogx_strerror(int status);
  *                      its 32 lanes per chunk of up to 32 targets (32 or 64; default 64).
  *                      64 lets a small leaf split its sources into more parts; it changes
  *                      the FP32 summation order of the near field only.
- * ogx_set_tuning applies from the next evaluation on; 0 in a field keeps its default. */
+ *   capture_steps    : 1 = ogx_step records a step as a CUDA graph and replays it (default 0).
+ *                      Such steps read no counts back in the middle: their launches and
+ *                      buffers are sized from capacities set by the last eager evaluation
+ *                      (counts plus an eighth).  The first step after the capacities were
+ *                      set runs without capture and sizes the buffers, the next is
+ *                      recorded, later ones replay it.  A step whose tree or lists exceed
+ *                      the capacities does nothing after its drift and is redone eagerly
+ *                      inside the same ogx_step call (new capacities, new capture), so the
+ *                      results are those of eager steps.  Each step ends with a host sync.
+ * ogx_set_tuning applies from the next evaluation on; 0 in a size field keeps its default. */
 typedef struct {
     int m2l_tile_targets;
     int near_units;
+    int capture_steps;
 } ogx_tuning;
 int ogx_set_tuning(void* handle, const ogx_tuning* t);
 int ogx_get_tuning(void* handle, ogx_tuning* out);

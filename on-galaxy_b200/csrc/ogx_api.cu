@@ -26,6 +26,11 @@ void set_last_error(int, const std::string& msg) { g_last_error = msg; }
 
 int Arena::get(Slot s, size_t bytes, void** out) {
     if (cap[s] < bytes) {
+        if (frozen) {
+            set_last_error(OGX_ERR_STATE, "a device buffer would grow while a step is captured");
+            return OGX_ERR_STATE;
+        }
+        ++generation;
         if (ptr[s]) {
             cudaFree(ptr[s]);
             total -= cap[s];
@@ -137,14 +142,43 @@ __global__ void k_drift(double* pos, const double* vel, const double* acc, int64
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < n3) pos[i] += vel[i] * dt + acc[i] * half_dt2;
 }
-__global__ void k_kick(double* vel, const double* acc_old, const double* acc_new, int64_t n3, double half_dt) {
+// v += (a_old + a_new) dt / 2, then a_old = a_new.  `counts` (capacity mode): a step
+// whose evaluation overflowed its capacities leaves v and a_old untouched, so the host
+// can redo the evaluation and the kick.
+__global__ void k_kick(double* vel, double* acc_old, const double* acc_new, int64_t n3, double half_dt,
+                       const DevCounts* counts) {
+    if (counts && counts->overflow) return;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n3) vel[i] += (acc_old[i] + acc_new[i]) * half_dt;
+    if (i < n3) {
+        vel[i] += (acc_old[i] + acc_new[i]) * half_dt;
+        acc_old[i] = acc_new[i];
+    }
 }
 
 static int device_error(Handle& h);
 
 static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot);
+static void counts_to_stats(Handle& h);
+
+// Capacities for capacity mode from the counts an eager evaluation read back (box and
+// leaf counts at sync point 1, list sizes at sync point 2): an eighth more, plus slack,
+// so the small changes of a step's tree fit; one more tree level; the sort depth used.
+static void update_capacity(Handle& h) {
+    const DevCounts& c = *h.h_counts;
+    Capacity& k = h.cap;
+    const Capacity old = k;
+    k.nb = (int)(c.num_boxes + c.num_boxes / 8 + 256);
+    k.nleaf = (int)(c.num_leaves + c.num_leaves / 8 + 256);
+    k.levels = std::min(kMaxDepth + 1, c.max_level + 2);
+    k.u = c.u_total + c.u_total / 8 + 4096;
+    k.w = c.w_total + c.w_total / 8 + 4096;
+    k.full_sort = h.full_sort_used;
+    k.valid = true;
+    // a captured step keeps the capacities it was captured with while its counts fit
+    if (old.valid && h.step_exec && c.num_boxes <= old.nb && c.num_leaves <= old.nleaf && c.max_level + 1 <= old.levels &&
+        c.u_total <= old.u && c.w_total <= old.w && (old.full_sort || !h.full_sort_used))
+        k = old;
+}
 
 // Every evaluation runs on the handle's internal high-priority stream: ordered
 // after the caller's stream's earlier work and before its later work.
@@ -169,26 +203,36 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     const int64_t l0 = h.launches;
     OGX_TRY(device_error(h));
     const cudaStream_t st = h.stream;
-    OGX_CUDA(cudaEventRecord(h.ev[0], st));
+    OGX_CUDA(timing_record(h, h.ev[0], st));
     if (h.prm.solver == OGX_SOLVER_DIRECT) {
         OGX_TRY(direct_eval(h, d_pos, d_mass, n, d_acc, d_pot, false));
-        OGX_CUDA(cudaEventRecord(h.ev[8], st));
+        OGX_CUDA(timing_record(h, h.ev[8], st));
         h.stats.launches = h.launches - l0;
         return OGX_OK;
     }
     OGX_TRY(ensure_operator_tables(h));
     OGX_TRY(tree_build(h, d_pos, d_mass, n));
-    OGX_CUDA(cudaEventRecord(h.ev[1], st));
+    OGX_CUDA(timing_record(h, h.ev[1], st));
     // mixed form: the upward pass needs only the tree, so it runs on its own stream
     // while the lists are built
     h.upward_split = (h.prm.precision == OGX_PREC_MIXED);
     if (h.upward_split) OGX_TRY(fmm_mixed_upward(h));
     OGX_TRY(lists_build(h));
-    OGX_CUDA(cudaEventRecord(h.ev[9], st));
+    OGX_CUDA(timing_record(h, h.ev[9], st));
     h.tree_valid = true;
+    // an eager evaluation has read its counts back by now: capacities for capacity mode
+    if (!h.cap_mode) update_capacity(h);
     if (h.prm.precision == OGX_PREC_MIXED) OGX_TRY(fmm_mixed(h, d_acc, d_pot));
     else OGX_TRY(fmm_fp64(h, d_acc, d_pot));   // the plain form, or with rotation-based M2L
-    OGX_CUDA(cudaEventRecord(h.ev[8], st));
+    // every count of this evaluation (the overflow flag included) reaches the host with it
+    OGX_CUDA(cudaMemcpyAsync(h.h_counts, h.d_counts, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(timing_record(h, h.ev[8], st));
+    h.stats.launches = h.launches - l0;
+    return OGX_OK;
+}
+
+// counts of the last evaluation (host copy, valid after a synchronize) into the stats
+static void counts_to_stats(Handle& h) {
     const DevCounts& c = *h.h_counts;
     h.stats.num_boxes = (int32_t)c.num_boxes;
     h.stats.num_leaves = (int32_t)c.num_leaves;
@@ -202,8 +246,6 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     h.stats.p2l_evals = c.p2l_evals;
     h.stats.adjacency_mismatch = c.adj_mismatch;
     h.stats.list_v = c.v_total;
-    h.stats.launches = h.launches - l0;
-    return OGX_OK;
 }
 
 // a bounded device wait that ran out in the previous evaluation (read after a sync)
@@ -234,6 +276,7 @@ static void finish_stats(Handle& h) {
     ogx_stats& s = h.stats;
     s.ms_total = ev_ms(h.ev[0], h.ev[8]);
     if (h.prm.solver == OGX_SOLVER_DIRECT) return;
+    counts_to_stats(h);
     s.ms_tree = ev_ms(h.ev[0], h.ev[1]);
     s.ms_lists = ev_ms(h.ev[1], h.ev[9]);
     s.ms_upward = ev_ms(h.ev[2], h.upward_split ? h.ev_up_end : h.ev[3]);
@@ -241,6 +284,61 @@ static void finish_stats(Handle& h) {
     s.ms_p2l = ev_ms(h.ev[4], h.ev[5]);
     s.ms_downward = ev_ms(h.ev[5], h.ev[6]);
     s.ms_leaf = ev_ms(h.ev[6], h.ev[7]);
+}
+
+// One leapfrog step (VelocityVerlet3D::step, src3d/Integrator3D.hpp:23-40) on h.stream:
+// drift, evaluation (eager, or sized by the capacities in capacity mode), kick.
+static int step_once(Handle& h, double* dp, double* dv, const double* dm, double* da, double* dn, double dt) {
+    const int64_t n3 = 3 * h.n;
+    const int grid = (int)((n3 + 255) / 256);
+    k_drift<<<grid, 256, 0, h.stream>>>(dp, dv, da, n3, dt, 0.5 * dt * dt); ++h.launches;
+    OGX_TRY(eval_device(h, h.n, dp, dm, dn, nullptr));
+    k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt, h.cap_mode ? h.d_counts : nullptr); ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+// Release the captured step (its buffers moved, its launch shapes changed, or a later
+// step did not fit its capacities).
+void drop_step_graph(Handle& h) {
+    if (h.step_exec) cudaGraphExecDestroy(h.step_exec);
+    if (h.step_graph) cudaGraphDestroy(h.step_graph);
+    h.step_exec = nullptr;
+    h.step_graph = nullptr;
+    h.cap_warm = 0;
+}
+
+// Record one step in capacity mode as a CUDA graph (nothing is launched).
+static int capture_step(Handle& h, double* dp, double* dv, const double* dm, double* da, double* dn, double dt) {
+    const int64_t l0 = h.launches;
+    OGX_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeRelaxed));
+    h.capturing = true;
+    h.cap_mode = true;
+    h.ws.frozen = true;
+    const int rc = step_once(h, dp, dv, dm, da, dn, dt);
+    h.ws.frozen = false;
+    h.cap_mode = false;
+    h.capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h.stream, &g);
+    if (rc != OGX_OK || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (rc != OGX_OK) return rc;
+        set_last_error(OGX_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ec));
+        return OGX_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&h.step_exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        h.step_exec = nullptr;
+        set_last_error(OGX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+        return OGX_ERR_CUDA;
+    }
+    h.step_graph = g;
+    h.step_launches = h.launches - l0;
+    h.step_gen = h.ws.generation;
+    return OGX_OK;
 }
 
 }  // namespace ogx
@@ -334,6 +432,7 @@ int ogx_destroy(void* handle) {
     {
         DeviceGuard g(h->device);
         cudaStreamSynchronize(h->stream);
+        drop_step_graph(*h);
         h->ws.release();
         if (h->h_counts) cudaFreeHost(h->h_counts);
         if (h->h_err) cudaFreeHost(h->h_err);
@@ -417,6 +516,8 @@ int ogx_last_stats(void* handle, ogx_stats* out) {
     HANDLE(handle);
     DeviceGuard g(h.device);
     if (h.stats.ms_total == 0.0) finish_stats(h);
+    h.stats.graph_steps = h.graph_steps;
+    h.stats.step_redos = h.overflow_redos;
     *out = h.stats;
     return OGX_OK;
 }
@@ -426,6 +527,7 @@ int ogx_upload(void* handle, int64_t n, const double* pos, const double* vel, co
     if (!handle || n <= 0 || !pos || !vel || !mass || n > (int64_t)INT32_MAX / 2) return OGX_ERR_INVALID;
     HANDLE(handle);
     DeviceGuard g(h.device);
+    drop_step_graph(h);   // a new system: new sizes and capacities
     double *dp, *dv, *dm, *da;
     OGX_TRY(arena_get(h.ws, S_POS, 3 * n, &dp));
     OGX_TRY(arena_get(h.ws, S_VEL, 3 * n, &dv));
@@ -453,13 +555,55 @@ int ogx_step(void* handle, double dt, int nsteps) {
     OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
     OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
     OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
-    const int grid = (int)((n3 + 255) / 256);
     for (int s = 0; s < nsteps; ++s) {
-        k_drift<<<grid, 256, 0, h.stream>>>(dp, dv, da, n3, dt, 0.5 * dt * dt); ++h.launches;
-        OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
-        k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt); ++h.launches;
-        OGX_CUDA(cudaMemcpyAsync(da, dn, n3 * sizeof(double), cudaMemcpyDeviceToDevice, h.stream));
-        h.stats.launches += 2;  // drift + kick around the evaluation
+        const bool graphed = h.capture_steps && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
+        if (!graphed) {
+            h.cap_mode = false;
+            OGX_TRY(step_once(h, dp, dv, dm, da, dn, dt));
+            h.stats.launches += 2;  // drift + kick around the evaluation
+            continue;
+        }
+        // Step capture: the first step after the capacities were set runs uncaptured
+        // in capacity mode (every buffer grows to its capacity there), the next one is
+        // recorded as a graph, and later steps replay it.  Each step copies its counts
+        // to the host; a step whose tree or lists overflowed did nothing after its
+        // drift and is redone eagerly here, which also sets new capacities.
+        if (h.step_exec && h.step_gen != h.ws.generation) drop_step_graph(h);
+        int64_t launched = 0;
+        if (h.step_exec) {
+            OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
+            h.launches += h.step_launches;
+            launched = h.step_launches;
+            ++h.graph_steps;
+        } else if (h.cap_warm == 0) {
+            const int64_t l0 = h.launches;
+            h.cap_mode = true;
+            const int rc = step_once(h, dp, dv, dm, da, dn, dt);
+            h.cap_mode = false;
+            OGX_TRY(rc);
+            h.cap_warm = 1;
+            launched = h.launches - l0;
+        } else {
+            OGX_TRY(capture_step(h, dp, dv, dm, da, dn, dt));
+            OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
+            launched = h.step_launches;
+            ++h.graph_steps;
+        }
+        OGX_CUDA(cudaStreamSynchronize(h.stream));
+        OGX_TRY(device_error(h));
+        if (h.h_counts->overflow) {
+            drop_step_graph(h);
+            h.cap_mode = false;
+            const int grid = (int)((n3 + 255) / 256);
+            OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
+            k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt, nullptr); ++h.launches;
+            OGX_CUDA(cudaGetLastError());
+            ++h.overflow_redos;
+            h.stats.launches += 1;
+        } else {
+            finish_stats(h);   // times and counts of the step that just ran
+            h.stats.launches = launched;
+        }
     }
     OGX_CUDA(cudaGetLastError());
     h.n = n;
@@ -491,14 +635,16 @@ int ogx_tree_sizes(void* handle, int64_t* sizes) {
     DeviceGuard g(h.device);
     OGX_CUDA(cudaStreamSynchronize(h.stream));
     const TreeView& tv = h.tv;
-    std::vector<int> col((size_t)27 * tv.nb), child((size_t)8 * tv.nb), parent(tv.nb);
+    // exact sizes (a step in capacity mode launched with capacities)
+    const int exact_nb = h.h_counts->nb32, exact_nl = h.h_counts->nleaf32;
+    std::vector<int> col((size_t)27 * exact_nb), child((size_t)8 * exact_nb), parent(exact_nb);
     OGX_CUDA(cudaMemcpy(col.data(), tv.col, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
     OGX_CUDA(cudaMemcpy(child.data(), tv.child, child.size() * sizeof(int), cudaMemcpyDeviceToHost));
     OGX_CUDA(cudaMemcpy(parent.data(), tv.parent, parent.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    std::vector<int> coord((size_t)3 * tv.nb);
+    std::vector<int> coord((size_t)3 * exact_nb);
     OGX_CUDA(cudaMemcpy(coord.data(), tv.coord, coord.size() * sizeof(int), cudaMemcpyDeviceToHost));
     int64_t ncol = 0, nv = 0;
-    for (int b = 0; b < tv.nb; ++b) {
+    for (int b = 0; b < exact_nb; ++b) {
         for (int d = 0; d < 27; ++d) ncol += col[27 * (size_t)b + d] >= 0;
         if (parent[b] < 0) continue;
         const int P = parent[b];
@@ -514,8 +660,8 @@ int ogx_tree_sizes(void* handle, int64_t* sizes) {
             }
         }
     }
-    sizes[0] = tv.nb;
-    sizes[1] = tv.nleaf;
+    sizes[0] = exact_nb;
+    sizes[1] = exact_nl;
     sizes[2] = ncol;
     sizes[3] = h.h_counts->u_total;
     sizes[4] = nv;
@@ -531,7 +677,9 @@ int ogx_tree_boxes(void* handle, int32_t* boxes, double* centers, int32_t* perm)
     DeviceGuard g(h.device);
     OGX_CUDA(cudaStreamSynchronize(h.stream));
     const TreeView& tv = h.tv;
-    const size_t nb = tv.nb;
+    // exact sizes (a step in capacity mode launched with capacities)
+    const int exact_nb = h.h_counts->nb32, exact_nl = h.h_counts->nleaf32;
+    const size_t nb = exact_nb;
     std::vector<int> level(nb), coord(3 * nb), parent(nb), leafid(nb), pfirst(nb), pcount(nb);
     OGX_CUDA(cudaMemcpy(level.data(), tv.level, nb * sizeof(int), cudaMemcpyDeviceToHost));
     OGX_CUDA(cudaMemcpy(coord.data(), tv.coord, 3 * nb * sizeof(int), cudaMemcpyDeviceToHost));
@@ -559,7 +707,9 @@ int ogx_tree_list(void* handle, int which, int64_t* off, int32_t* idx) {
     DeviceGuard g(h.device);
     OGX_CUDA(cudaStreamSynchronize(h.stream));
     const TreeView& tv = h.tv;
-    const size_t nb = tv.nb, nl = tv.nleaf;
+    // exact sizes (a step in capacity mode launched with capacities)
+    const int exact_nb = h.h_counts->nb32, exact_nl = h.h_counts->nleaf32;
+    const size_t nb = exact_nb, nl = exact_nl;
     if (which == 0 || which == 2) {
         std::vector<int> col(27 * nb), child(8 * nb), parent(nb), coord(3 * nb);
         OGX_CUDA(cudaMemcpy(col.data(), tv.col, col.size() * sizeof(int), cudaMemcpyDeviceToHost));
@@ -628,8 +778,10 @@ int ogx_set_tuning(void* handle, const ogx_tuning* t) {
         set_last_error(OGX_ERR_INVALID, "ogx_set_tuning: m2l_tile_targets must be 32, 64, 96 or 128 and near_units 32 or 64");
         return OGX_ERR_INVALID;
     }
+    if (fill != h.tile_fill || units != h.near_units || (t->capture_steps != 0) != h.capture_steps) drop_step_graph(h);
     h.tile_fill = fill;
     h.near_units = units;
+    h.capture_steps = t->capture_steps != 0;
     return OGX_OK;
 }
 
@@ -638,6 +790,7 @@ int ogx_get_tuning(void* handle, ogx_tuning* out) {
     HANDLE(handle);
     out->m2l_tile_targets = h.tile_fill;
     out->near_units = h.near_units;
+    out->capture_steps = h.capture_steps ? 1 : 0;
     return OGX_OK;
 }
 

@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(128) k_p2x(TreeView tv, int ntargets, double* 
     extern __shared__ __align__(16) unsigned char s_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int t = blockIdx.x * 4 + wid;
-    if (t >= ntargets) return;
+    if (t >= ntargets || t >= (MODE == 0 ? tv_nleaf(tv) : tv_nb(tv)) || tv_over(tv)) return;
     T* buf = reinterpret_cast<T*>(s_raw) + (size_t)wid * 32 * LD;
     const int b = (MODE == 0) ? tv.leafbox[t] : t;
     int64_t e0, e1;
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(128) k_eval_coeffs(TreeView tv, int count, con
     using Lo = EvalLayout<P>;
     const int lane = threadIdx.x & 31;
     const int k = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (k >= count) return;
+    if (k >= count || k >= (MODE == 0 ? tv_nb(tv) : tv_nleaf(tv)) || tv_over(tv)) return;
     const int b = (MODE == 0) ? k : tv.leafbox[k];
     if (MODE == 0 && tv.x_off[b] == tv.x_off[b + 1]) return;
     const double* c = coef + (size_t)b * Lo::K;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128) k_leaf_far(TreeView tv, const T* __restri
     __shared__ T s_rec[4][Lo::HREC > Lo::GREC ? Lo::HREC : Lo::GREC];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * 4 + wid;
-    if (lf >= tv.nleaf) return;
+    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
     T* sr = s_rec[wid];
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];

@@ -106,92 +106,104 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
     __shared__ double s_in[MODE == 0 ? 8 : 1][TR_PB][K];
     __shared__ double s_part[MODE == 0 ? 8 : 1][TR_PB][MODE == 0 ? K : 1];
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
-    // this level's non-leaf parents (count known on the device only; the grid is
-    // sized for all boxes of the level)
+    // this level's non-leaf parents (count known on the device only): the CTAs take
+    // groups of TR_PB parents in turn
+    if (tv_over(tv)) return;
     const int first = nl_off[level], count = nl_off[level + 1] - first;
     const int* parents = nonleaf + first;
-    const int p0 = blockIdx.x * TR_PB;
-    if (p0 >= count) return;
-    int bx[TR_PB], ch[TR_PB];
-    bool any = false;
+    for (int p0 = blockIdx.x * TR_PB; p0 < count; p0 += gridDim.x * TR_PB) {
+        if (MODE == 0) __syncthreads();   // s_part of the previous group is read
+        int bx[TR_PB], ch[TR_PB];
+        bool any = false;
 #pragma unroll
-    for (int a = 0; a < TR_PB; ++a) {
-        bx[a] = (p0 + a < count) ? parents[p0 + a] : -1;
-        ch[a] = (bx[a] >= 0) ? tv.child[8 * bx[a] + s] : -1;
-        any |= ch[a] >= 0;
-    }
-    if (MODE == 0) {
+        for (int a = 0; a < TR_PB; ++a) {
+            bx[a] = (p0 + a < count) ? parents[p0 + a] : -1;
+            ch[a] = (bx[a] >= 0) ? tv.child[8 * bx[a] + s] : -1;
+            any |= ch[a] >= 0;
+        }
+        if (MODE == 0) {
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a)
+                for (int d = lane; d < K; d += 32) s_in[s][a][d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
+            __syncwarp();
+        } else {
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a)
+                for (int d = threadIdx.x; d < K; d += blockDim.x) s_in[0][a][d] = (bx[a] >= 0) ? local[(size_t)bx[a] * K + d] : 0.0;
+            __syncthreads();
+        }
+        double acc[TR_PB][NPL];
 #pragma unroll
         for (int a = 0; a < TR_PB; ++a)
-            for (int d = lane; d < K; d += 32) s_in[s][a][d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
-        __syncwarp();
-    } else {
 #pragma unroll
-        for (int a = 0; a < TR_PB; ++a)
-            for (int d = threadIdx.x; d < K; d += blockDim.x) s_in[0][a][d] = (bx[a] >= 0) ? local[(size_t)bx[a] * K + d] : 0.0;
-        __syncthreads();
-    }
-    double acc[TR_PB][NPL];
-#pragma unroll
-    for (int a = 0; a < TR_PB; ++a)
-#pragma unroll
-        for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
-    if (any) {  // warp-uniform
-        const double* T = opsT + (size_t)s * K * K;
-        const int si = MODE == 0 ? s : 0;
+            for (int q = 0; q < NPL; ++q) acc[a][q] = 0.0;
+        if (any) {  // warp-uniform
+            const double* T = opsT + (size_t)s * K * K;
+            const int si = MODE == 0 ? s : 0;
 #pragma unroll 8
-        for (int kk = 0; kk < K; ++kk) {
-            double tq[NPL];
+            for (int kk = 0; kk < K; ++kk) {
+                double tq[NPL];
 #pragma unroll
-            for (int q = 0; q < NPL; ++q) {
-                const int j = lane + 32 * q;
-                tq[q] = (j < K) ? __ldg(T + (size_t)kk * K + j) : 0.0;
+                for (int q = 0; q < NPL; ++q) {
+                    const int j = lane + 32 * q;
+                    tq[q] = (j < K) ? __ldg(T + (size_t)kk * K + j) : 0.0;
+                }
+#pragma unroll
+                for (int a = 0; a < TR_PB; ++a) {
+                    const double v = s_in[si][a][kk];
+#pragma unroll
+                    for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
+                }
             }
+        }
+        if (MODE == 1) {
 #pragma unroll
             for (int a = 0; a < TR_PB; ++a) {
-                const double v = s_in[si][a][kk];
+                if (ch[a] < 0) continue;
 #pragma unroll
-                for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
+                for (int q = 0; q < NPL; ++q) {
+                    const int j = lane + 32 * q;
+                    if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a)
+#pragma unroll
+                for (int q = 0; q < NPL; ++q) {
+                    const int j = lane + 32 * q;
+                    if (j < K) s_part[s][a][j] = acc[a][q];
+                }
+            __syncthreads();
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a) {
+                if (bx[a] < 0) continue;
+                for (int d = threadIdx.x; d < K; d += blockDim.x) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int o = 0; o < 8; ++o) v += s_part[o][a][d];
+                    mpole[(size_t)bx[a] * K + d] = v;
+                }
             }
         }
+        if (MODE == 1) __syncthreads();   // s_in is refilled for the next group
     }
-    if (MODE == 1) {
-#pragma unroll
-        for (int a = 0; a < TR_PB; ++a) {
-            if (ch[a] < 0) continue;
-#pragma unroll
-            for (int q = 0; q < NPL; ++q) {
-                const int j = lane + 32 * q;
-                if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
-            }
-        }
-    } else {
-#pragma unroll
-        for (int a = 0; a < TR_PB; ++a)
-#pragma unroll
-            for (int q = 0; q < NPL; ++q) {
-                const int j = lane + 32 * q;
-                if (j < K) s_part[s][a][j] = acc[a][q];
-            }
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < TR_PB; ++a) {
-            if (bx[a] < 0) continue;
-            for (int d = threadIdx.x; d < K; d += blockDim.x) {
-                double v = 0.0;
-#pragma unroll
-                for (int o = 0; o < 8; ++o) v += s_part[o][a][d];
-                mpole[(size_t)bx[a] * K + d] = v;
-            }
-        }
-    }
+}
+
+// CTAs of one level's translation: enough for the level's boxes (eager: the level
+// size is known on the host), or a fixed grid that walks the level (capacity mode)
+template <int P>
+int translate_grid(const Handle& h, int l) {
+    if (h.cap_mode) return 2 * h.num_sms;
+    const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
+    return (nbl + tr_pb<P>() - 1) / tr_pb<P>();
 }
 
 template <int P>
 int launch_m2m(Handle& h, double* M) {
     for (int l = h.max_level - 1; l >= 0; --l) {
-        const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
-        if (nbl > 0) { k_translate_oct<P, 0><<<(nbl + tr_pb<P>() - 1) / tr_pb<P>(), 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
+        const int g = translate_grid<P>(h, l);
+        if (g > 0) { k_translate_oct<P, 0><<<g, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -200,11 +212,10 @@ template <int P>
 int launch_l2l(Handle& h, double* L, const double* Lown) {
     constexpr int K = (P + 1) * (P + 1);
     // root (no parent): its local is its own M2L/P2L part
-    OGX_CUDA(cudaMemcpyAsync(L + (size_t)h.level_off[0] * K, Lown + (size_t)h.level_off[0] * K, sizeof(double) * K,
-                             cudaMemcpyDeviceToDevice, h.stream));
+    OGX_CUDA(cudaMemcpyAsync(L, Lown, sizeof(double) * K, cudaMemcpyDeviceToDevice, h.stream));   // box 0 is the root
     for (int l = 0; l < h.max_level; ++l) {
-        const int nbl = h.level_off[l + 1] - h.level_off[l];
-        if (nbl > 0) { k_translate_oct<P, 1><<<(nbl + tr_pb<P>() - 1) / tr_pb<P>(), 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
+        const int g = translate_grid<P>(h, l);
+        if (g > 0) { k_translate_oct<P, 1><<<g, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
     }
     return OGX_OK;
 }
@@ -227,6 +238,7 @@ __global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uin
     __shared__ int s_t;
     const int tid = threadIdx.x;
     const int base = blockIdx.x * M2L_TGT;
+    if (tv_over(tv)) return;
     // the padded target layout never mixes octants inside a tile
     if (tid == 0) s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
     __syncthreads();
@@ -299,7 +311,7 @@ template <bool POT>
 __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * 4 + wid;
-    if (lf >= tv.nleaf) return;
+    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     for (int j0 = 0; j0 < cnt; j0 += 32) {
@@ -346,14 +358,14 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
     OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
     OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
-    OGX_CUDA(cudaEventRecord(h.ev[2], st));
+    OGX_CUDA(timing_record(h, h.ev[2], st));
     // upward
     const size_t p2x_smem = p2x_smem_bytes<P, double>();
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 0, double>, (int)p2x_smem));
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, double>, (int)p2x_smem));
     k_p2x<P, 0, double><<<(tv.nleaf + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nleaf, M); ++h.launches;
     OGX_TRY(launch_m2m<P>(h, M));
-    OGX_CUDA(cudaEventRecord(h.ev[3], st));
+    OGX_CUDA(timing_record(h, h.ev[3], st));
     // M2L
     OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
     if (h.ntgt > 0 && h.prm.precision == OGX_PREC_FP64_ROT) {
@@ -365,20 +377,20 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
         const int ntiles = h.ntgt_pad / M2L_TGT;
         k_m2l_fp64<P><<<ntiles, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M, Lown); ++h.launches;
     }
-    OGX_CUDA(cudaEventRecord(h.ev[4], st));
+    OGX_CUDA(timing_record(h, h.ev[4], st));
     // P2L
     k_p2x<P, 1, double><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches;
-    OGX_CUDA(cudaEventRecord(h.ev[5], st));
+    OGX_CUDA(timing_record(h, h.ev[5], st));
     // L2L top-down
     OGX_TRY(launch_l2l<P>(h, L, Lown));
-    OGX_CUDA(cudaEventRecord(h.ev[6], st));
+    OGX_CUDA(timing_record(h, h.ev[6], st));
     // leaves
     const bool pot = d_pot != nullptr;
     OGX_TRY((launch_far<P, double>(h, M, L, far, pot)));
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
     if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
     else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
-    OGX_CUDA(cudaEventRecord(h.ev[7], st));
+    OGX_CUDA(timing_record(h, h.ev[7], st));
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
@@ -494,15 +506,15 @@ int run_mixed_upward(Handle& h) {
     const cudaStream_t main_st = h.stream, su = h.up;
     OGX_CUDA(cudaStreamWaitEvent(su, h.ev_tree, 0));
     h.stream = su;   // launch_m2m issues on h.stream
-    OGX_CUDA(cudaEventRecord(h.ev[2], su));
+    OGX_CUDA(timing_record(h, h.ev[2], su));
     k_p2x<P, 0, float><<<(tv.nleaf + 3) / 4, 128, p2x_smem, su>>>(tv, tv.nleaf, M); ++h.launches;
     const int rc = launch_m2m<P>(h, M);
     h.stream = main_st;
     OGX_TRY(rc);
     if constexpr (C::SUPPORTED) {
-        mixed::k_split_mpole<P><<<(tv.nb + 3) / 4, 128, 0, su>>>(M, tv.nb, mhi, mlo, mus); ++h.launches;
+        mixed::k_split_mpole<P><<<(tv.nb + 3) / 4, 128, 0, su>>>(M, tv.nb, mhi, mlo, mus, tv.cnt); ++h.launches;
     }
-    OGX_CUDA(cudaEventRecord(h.ev_up_end, su));
+    OGX_CUDA(timing_record(h, h.ev_up_end, su));
     OGX_CUDA(cudaEventRecord(h.ev_up, su));
     return OGX_OK;
 }
@@ -530,7 +542,7 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
     // join the upward pass
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
-    OGX_CUDA(cudaEventRecord(h.ev[3], st));
+    OGX_CUDA(timing_record(h, h.ev[3], st));
     // the near field needs only the tree and the lists: it may start with the M2L
     OGX_CUDA(cudaEventRecord(h.ev_fork, st));
     // M2L on the tensor cores
@@ -567,20 +579,20 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches;
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
-    OGX_CUDA(cudaEventRecord(h.ev[4], st));
+    OGX_CUDA(timing_record(h, h.ev[4], st));
     if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }
     else { k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches; }
-    OGX_CUDA(cudaEventRecord(h.ev[5], st));
+    OGX_CUDA(timing_record(h, h.ev[5], st));
     OGX_TRY(launch_l2l<P>(h, L, Lown));
-    OGX_CUDA(cudaEventRecord(h.ev[6], st));
+    OGX_CUDA(timing_record(h, h.ev[6], st));
     const bool pot = d_pot != nullptr;
     OGX_TRY(launch_far32<P>(h, M, L, far, pot));
     // join the near field, then acc = G (far + near) in the caller's order
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_join, 0));
     const double G = h.prm.G;
-    if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, d_pot); ++h.launches; }
-    else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, nullptr); ++h.launches; }
-    OGX_CUDA(cudaEventRecord(h.ev[7], st));
+    if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, d_pot, tv.cnt); ++h.launches; }
+    else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, nullptr, tv.cnt); ++h.launches; }
+    OGX_CUDA(timing_record(h, h.ev[7], st));
     OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;

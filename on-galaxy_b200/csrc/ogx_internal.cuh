@@ -87,6 +87,8 @@ struct Arena {
     void* ptr[S_NUM_SLOTS] = {};
     size_t cap[S_NUM_SLOTS] = {};
     size_t total = 0;
+    uint64_t generation = 0;   // bumped by every (re)allocation: a captured step's buffers moved
+    bool frozen = false;       // while a step is captured: growing a slot is an error
     int get(Slot s, size_t bytes, void** out);
     void release();
 };
@@ -136,7 +138,12 @@ struct RootInfo {
     int pad;
 };
 
-// counts produced on the device and read back at the two host sync points
+// Counts produced on the device.  An eager evaluation reads them back at two host sync
+// points (box count, list sizes) to size what follows; an evaluation in capacity mode
+// (no read-back, so a step can be captured as a CUDA graph) sizes its launches and
+// buffers from capacities instead, and every kernel takes its bounds from these device
+// counts.  `overflow` is set when a count exceeds its capacity: every later kernel of the
+// evaluation then does nothing and the host redoes the evaluation eagerly.
 struct DevCounts {
     int64_t num_boxes;
     int64_t num_leaves;
@@ -151,12 +158,18 @@ struct DevCounts {
     int32_t pad_err;
     int32_t nonleaf_level[kMaxDepth + 2];
     int32_t deep_flag;   // some level-16 box holds more than leaf_capacity bodies
-    int32_t pad_deep;
+    int32_t overflow;    // capacity mode: a count above its capacity (see above)
+    int32_t nb32, nleaf32;   // num_boxes, num_leaves
+    int32_t ntgt32;          // M2L targets (boxes of level >= 2)
+    int32_t pad_cnt;
 };
 
-// device view of the tree handed to kernels
+// device view of the tree handed to kernels.  nb and nleaf size the launches (the exact
+// counts in an eager evaluation, the capacities in capacity mode); kernels bound their
+// work by the device counts in `cnt` (tv_nb, tv_nleaf), which are always exact.
 struct TreeView {
     int n, nb, nleaf;
+    const DevCounts* cnt;
     const RootInfo* root;
     const double *px, *py, *pz, *pm;   // sorted bodies
     const int* perm;                   // sorted -> original
@@ -174,6 +187,21 @@ struct TreeView {
     const int *u_idx, *w_idx;
     const int64_t* x_off;              // per box (nb+1)
     const int* x_idx;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ int tv_nb(const TreeView& tv) { return tv.cnt->nb32; }
+__device__ __forceinline__ int tv_nleaf(const TreeView& tv) { return tv.cnt->nleaf32; }
+__device__ __forceinline__ bool tv_over(const TreeView& tv) { return tv.cnt->overflow != 0; }
+#endif
+
+// launch sizes of an evaluation in capacity mode, from an earlier eager evaluation
+struct Capacity {
+    int nb = 0, nleaf = 0;
+    int levels = 0;          // tree levels 0 .. levels-1 are walked by the translations
+    int64_t u = 0, w = 0;    // U- and W-list entries
+    bool full_sort = false;  // sort all 24 key levels (the tree had a deep cluster)
+    bool valid = false;
 };
 
 struct Handle {
@@ -220,6 +248,21 @@ struct Handle {
     float* d_tc_ounscale = nullptr; // per M2L operator: 2^e undoing the scaling of its FP16 images
     int* d_err = nullptr;          // device error word of the bounded waits
     int* h_err = nullptr;          // pinned copy
+    // capacity mode and the captured step (ogx_step with step capture on)
+    bool cap_mode = false;        // this evaluation sizes its launches from `cap`
+    bool full_sort_used = false;  // the last tree build sorted all 24 key levels
+    Capacity cap;
+    bool capture_steps = false;   // ogx_set_tuning: replay each step as a CUDA graph
+    bool capturing = false;       // a capture is being recorded on h.stream
+    int cap_warm = 0;             // capacity-mode steps run since `cap` was set
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    int64_t step_launches = 0;    // kernels in one captured step
+    uint64_t step_gen = 0;        // arena generation the captured step was recorded with
+    int64_t overflow_redos = 0;   // steps redone eagerly after an overflow
+    int64_t graph_steps = 0;      // steps replayed from the captured graph
+    DevCounts* d_counts = nullptr;   // the counts of the last evaluation (device)
+    int* d_level_off = nullptr;      // first box of every level (device, kMaxDepth + 2)
     // launch-shape knobs (ogx_set_tuning)
     int tile_fill = 128;    // targets per 128-row M2L tile
     int near_units = 64;    // (target, source part) units per near-field chunk
@@ -234,6 +277,13 @@ struct Handle {
     const int* d_nonleaf = nullptr;
     const int* d_nonleaf_off = nullptr;   // device, kMaxDepth + 2 entries
 };
+
+// A timing event of the evaluation.  While a step is being captured as a CUDA graph
+// the record must become an event-record node of the graph (cudaEventRecordExternal);
+// a plain record on a capturing stream would only mark a capture dependency.
+inline cudaError_t timing_record(const Handle& h, cudaEvent_t e, cudaStream_t st) {
+    return cudaEventRecordWithFlags(e, st, h.capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
 
 // ---- host-side operator tables (ogx_tables.cpp) -----------------------------
 // kind 0: M2M for child octant index (0..7), maps child M' -> parent M'
@@ -256,6 +306,7 @@ int fmm_mixed_upward(Handle& h);   // upward pass on h.up, right after the tree 
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);
+void drop_step_graph(Handle& h);   // ogx_api.cu
 int eval_device_shared(Handle& h, int64_t n, const double* d_pos, const double* d_mass, double* d_acc, double* d_pot);
 void finish_stats_shared(Handle& h);
 int direct_launch(const double* d_pos, const double* d_mass, int64_t n, double G, double eps2, double* d_acc, double* d_pot,

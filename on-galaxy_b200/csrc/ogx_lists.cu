@@ -29,10 +29,6 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int UW_STACK = 192;
 
-struct LevelOffsets {
-    int off[kMaxDepth + 2];   // first box of each level, off[l + 1] = end of level l
-};
-
 // p's highest set bit is below q's
 __device__ __forceinline__ bool msb_less(unsigned p, unsigned q) { return p < q && p < (p ^ q); }
 
@@ -48,19 +44,21 @@ __device__ __forceinline__ bool morton_less(int ax, int ay, int az, int bx, int 
     return d == 0 ? ax < bx : (d == 1 ? ay < by : az < bz);
 }
 
-// colleague slot d of box b: the box of b's level at integer offset (d % 3 - 1, ...)
-__global__ void k_colleagues_bs(int nb, LevelOffsets lv, const int* __restrict__ level, const int* __restrict__ coord,
-                                int* __restrict__ col) {
+// colleague slot d of box b: the box of b's level at integer offset (d % 3 - 1, ...);
+// level_off[l] = first box of level l (device)
+__global__ void k_colleagues_bs(int nb_cap, const int* __restrict__ level_off, const int* __restrict__ level,
+                                const int* __restrict__ coord, int* __restrict__ col, const DevCounts* counts) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= 27 * (int64_t)nb) return;
+    if (t >= 27 * (int64_t)nb_cap || counts->overflow) return;
     const int b = (int)(t / 27), d = (int)(t - 27 * (int64_t)b);
+    if (b >= counts->nb32) { col[t] = -1; return; }
     if (d == 13) { col[t] = b; return; }
     const int l = level[b];
     const int side = 1 << l;
     const int nx = coord[3 * b] + d % 3 - 1, ny = coord[3 * b + 1] + (d / 3) % 3 - 1, nz = coord[3 * b + 2] + d / 9 - 1;
     int found = -1;
     if (l > 0 && nx >= 0 && ny >= 0 && nz >= 0 && nx < side && ny < side && nz < side) {
-        int lo = lv.off[l], hi = lv.off[l + 1] - 1;
+        int lo = level_off[l], hi = level_off[l + 1] - 1;
         while (lo <= hi) {
             const int mid = (lo + hi) >> 1;
             const int mx = coord[3 * mid], my = coord[3 * mid + 1], mz = coord[3 * mid + 2];
@@ -81,7 +79,7 @@ __global__ void __launch_bounds__(128) k_colleagues_check(int first, int count, 
     __shared__ double s_kc[4][8][4];   // centres (x, y, z, half) of each warp's parent's children
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = blockIdx.x * 4 + wid;
-    if (k >= count) return;
+    if (k >= count || first + k >= counts->nb32 || counts->overflow) return;
     const int P = first + k;
     if (leafid[P] >= 0) return;
     int kids[8];
@@ -152,7 +150,7 @@ __global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restric
                                                  int* widx, DevCounts* counts) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * 4 + wid;
-    if (lf >= nleaf) return;
+    if (lf >= nleaf || lf >= counts->nleaf32 || counts->overflow) return;
     const int b = leafbox[lf];
     const double tol = root->tol;
     // adjacent64(ctr, a, b, tol) with b's centre held in registers
@@ -231,9 +229,9 @@ __global__ void __launch_bounds__(128) k_uw_warp(int nleaf, const int* __restric
 
 // X = transpose of W: emit (w, leaf box) in leaf order, count members per box
 __global__ void k_x_emit(int nleaf, const int* leafbox, const int64_t* woff, const int* widx, uint32_t* xkey, uint32_t* xval,
-                         int* xcnt) {
+                         int* xcnt, const DevCounts* counts) {
     const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lf >= nleaf) return;
+    if (lf >= nleaf || lf >= counts->nleaf32 || counts->overflow) return;
     const int b = leafbox[lf];
     for (int64_t e = woff[lf]; e < woff[lf + 1]; ++e) {
         xkey[e] = (uint32_t)widx[e];
@@ -249,10 +247,20 @@ __global__ void k_x_emit(int nleaf, const int* leafbox, const int64_t* woff, con
 // pattern then share tiles, so a tile runs fewer (colleague, child) combinations and
 // fewer of its operand rows are empty (on the 1M merger: 17% fewer combinations).  The
 // order of a tile's targets does not change any target's result.
-__global__ void k_tgt_keys(int first, int nb, const int* __restrict__ coord, const int* __restrict__ parent,
-                           const int* __restrict__ col, const int* __restrict__ child, uint32_t* key, uint32_t* val) {
+// Launched over the capacity of boxes: the targets are boxes level_off[2] .. nb - 1
+// (device counts); slots behind them get key 1 << 30 and sort after every target.
+__global__ void k_tgt_keys(int cap, const int* __restrict__ level_off, const int* __restrict__ coord,
+                           const int* __restrict__ parent, const int* __restrict__ col, const int* __restrict__ child,
+                           uint32_t* key, uint32_t* val, DevCounts* counts) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nb - first) return;
+    if (k >= cap || counts->overflow) return;
+    const int first = level_off[2], ntgt = counts->nb32 - first;
+    if (k == 0) counts->ntgt32 = ntgt;
+    if (k >= ntgt) {
+        key[k] = 1u << 30;
+        val[k] = 0xFFFFFFFFu;
+        return;
+    }
     const int b = first + k;
     const int tx = coord[3 * b] & 1, ty = coord[3 * b + 1] & 1, tz = coord[3 * b + 2] & 1;
     const int par = parent[b];
@@ -277,9 +285,10 @@ __global__ void k_tgt_keys(int first, int nb, const int* __restrict__ coord, con
 // bits 27-29): every octant group starts on a multiple of `tile`, so a tile never
 // mixes octants.  gs[0..8] = group starts,
 // gs[9..17] = padded group starts.
-__global__ void k_target_groups(const uint32_t* key, int ntgt, int tile, int fill, int* gs) {
+__global__ void k_target_groups(const uint32_t* key, const DevCounts* counts, int tile, int fill, int* gs) {
     __shared__ int lo_s[9];
     const int g = threadIdx.x;
+    const int ntgt = counts->overflow ? 0 : counts->ntgt32;
     if (g <= 8) {
         int lo = 0, hi = ntgt;  // first index with key >= g
         while (lo < hi) {
@@ -319,6 +328,21 @@ __global__ void k_target_pad(const uint32_t* box, const int* gs, int npad, int t
 }
 
 
+// list totals (the last entry of each exclusive scan over the leaf capacity, whose
+// padding counts are zero), checked against the capacities of the index arrays
+__global__ void k_check_lists(DevCounts* counts, const int64_t* utot, const int64_t* wtot, int64_t cap_u, int64_t cap_w) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    counts->u_total = *utot;
+    counts->w_total = *wtot;
+    if (*utot > cap_u || *wtot > cap_w) counts->overflow = 1;
+}
+
+// X-list keys behind the W total (device) get `v` and sort last
+__global__ void k_fill_tail_x(uint32_t* a, const DevCounts* counts, int64_t cap, uint32_t v) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < cap && k >= counts->w_total) a[k] = v;
+}
+
 inline int grid_for(int64_t n, int b) { return (int)((n + b - 1) / b); }
 inline int bits_for(int64_t v) {
     int b = 1;
@@ -331,14 +355,11 @@ inline int bits_for(int64_t v) {
 int lists_build(Handle& h) {
     const cudaStream_t st = h.stream;
     TreeView& tv = h.tv;
-    const int nb = tv.nb, nleaf = tv.nleaf;
-    DevCounts* dc;
-    OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
+    const int nb = tv.nb, nleaf = tv.nleaf;   // launch sizes (capacities in capacity mode)
+    DevCounts* dc = h.d_counts;
     int* col;
     OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
-    LevelOffsets lv{};
-    for (int l = 0; l <= h.max_level + 1 && l < kMaxDepth + 2; ++l) lv.off[l] = h.level_off[std::min<int>(l, (int)h.level_off.size() - 1)];
-    k_colleagues_bs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, st>>>(nb, lv, tv.level, tv.coord, col); ++h.launches;
+    k_colleagues_bs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, st>>>(nb, h.d_level_off, tv.level, tv.coord, col, dc); ++h.launches;
     k_colleagues_check<<<grid_for(nb, 4), 128, 0, st>>>(0, nb, tv.leafid, tv.child, tv.center, tv.root, col, dc); ++h.launches;
     tv.col = col;
 
@@ -349,6 +370,10 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_UW_LANE, 64 * (size_t)nleaf, &lane_uw));
     OGX_TRY(arena_get(h.ws, S_U_OFF, nleaf + 1, &uoff));
     OGX_TRY(arena_get(h.ws, S_W_OFF, nleaf + 1, &woff));
+    if (h.cap_mode) {   // padding leaves count nothing
+        OGX_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(int) * (size_t)nleaf, st));
+        OGX_CUDA(cudaMemsetAsync(wcnt, 0, sizeof(int) * (size_t)nleaf, st));
+    }
     int* lane_u = lane_uw;
     int* lane_w = lane_uw + 32 * (size_t)nleaf;
     k_uw_warp<false><<<grid_for(nleaf, 4), 128, 0, st>>>(nleaf, tv.leafbox, tv.parent, tv.child, tv.leafid, col, tv.center,
@@ -356,12 +381,19 @@ int lists_build(Handle& h) {
                                                          nullptr, nullptr, dc); ++h.launches;
     OGX_TRY(scan_i32_to_i64(h, ucnt, uoff, nleaf));
     OGX_TRY(scan_i32_to_i64(h, wcnt, woff, nleaf));
-    // sync point 2: list sizes
-    OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->u_total, uoff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaMemcpyAsync(&h.h_counts->w_total, woff + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-    OGX_CUDA(cudaStreamSynchronize(st));
-    const int64_t nu = h.h_counts->u_total, nw = h.h_counts->w_total;
+    int64_t nu, nw;
+    if (h.cap_mode) {
+        nu = h.cap.u;
+        nw = h.cap.w;
+        k_check_lists<<<1, 32, 0, st>>>(dc, uoff + nleaf, woff + nleaf, nu, nw); ++h.launches;
+    } else {
+        // sync point 2: list sizes
+        k_check_lists<<<1, 32, 0, st>>>(dc, uoff + nleaf, woff + nleaf, INT64_MAX, INT64_MAX); ++h.launches;
+        OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+        OGX_CUDA(cudaStreamSynchronize(st));
+        nu = h.h_counts->u_total;
+        nw = h.h_counts->w_total;
+    }
     int *uidx, *widx;
     OGX_TRY(arena_get(h.ws, S_U_IDX, nu + 1, &uidx));
     OGX_TRY(arena_get(h.ws, S_W_IDX, nw + 1, &widx));
@@ -370,7 +402,9 @@ int lists_build(Handle& h) {
                                                         widx, dc); ++h.launches;
     tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
 
-    // X lists
+    // X lists: W transposed by a stable sort on the W member; keys behind the W total
+    // (capacity padding) sort last and are never referenced by x_off
+    const int xbits = bits_for(nb);
     uint32_t *xk, *xv;
     int* xcnt;
     int64_t* xoff;
@@ -379,42 +413,40 @@ int lists_build(Handle& h) {
     OGX_TRY(arena_get(h.ws, S_X_CNT, nb, &xcnt));
     OGX_TRY(arena_get(h.ws, S_X_OFF, nb + 1, &xoff));
     OGX_CUDA(cudaMemsetAsync(xcnt, 0, sizeof(int) * (size_t)nb, st));
-    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt); ++h.launches;
+    k_x_emit<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, woff, widx, xk, xv, xcnt, dc); ++h.launches;
+    if (h.cap_mode) { k_fill_tail_x<<<grid_for(nw, 256), 256, 0, st>>>(xk, dc, nw, (1u << xbits) - 1u); ++h.launches; }
     uint32_t *xk_s, *xv_s;
-    OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, bits_for(nb), &xk_s, &xv_s));
+    OGX_TRY(radix_sort_u32(h, S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, nw, xbits, &xk_s, &xv_s));
     OGX_TRY(scan_i32_to_i64(h, xcnt, xoff, nb));
     tv.x_off = xoff;
     tv.x_idx = (const int*)xv_s;
 
-    // M2L targets grouped by child octant (levels >= 2)
-    const int first2 = (h.max_level >= 2) ? h.level_off[2] : nb;
-    const int ntgt = nb - first2;
+    // M2L targets (levels >= 2) grouped by child octant, then by the slot pattern of
+    // their V lists; launched over the box capacity, the padding sorts last
+    const int tcap = std::max(nb, 1);
     uint32_t *tk, *tb;
-    OGX_TRY(arena_get(h.ws, S_TGT_KEY, ntgt + 1, &tk));
-    OGX_TRY(arena_get(h.ws, S_TGT_BOX, ntgt + 1, &tb));
-    if (ntgt > 0) {
-        k_tgt_keys<<<grid_for(ntgt, 256), 256, 0, st>>>(first2, nb, tv.coord, tv.parent, col, tv.child, tk, tb); ++h.launches;
-        uint32_t *tk_s, *tb_s;
-        OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, ntgt, 30, &tk_s, &tb_s));
-        h.tgt_key = tk_s;
-        h.tgt_box = tb_s;
-        const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
-        const int fill = h.tile_fill;   // targets per tile (the M2L batch width)
-        const int npad = ((ntgt + fill - 1) / fill + 8) * tile;
-        int* gs;
-        uint32_t *pk, *pb;
-        OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
-        OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
-        OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
-        k_target_groups<<<1, 32, 0, st>>>(tk_s, ntgt, tile, fill, gs); ++h.launches;
-        k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, tile, fill, pk, pb); ++h.launches;
-        h.tgt_tile_key = pk;
-        h.tgt_tile_box = pb;
-        h.ntgt_pad = npad;
-    } else {
-        h.ntgt_pad = 0;
-    }
-    h.ntgt = ntgt;
+    OGX_TRY(arena_get(h.ws, S_TGT_KEY, tcap + 1, &tk));
+    OGX_TRY(arena_get(h.ws, S_TGT_BOX, tcap + 1, &tb));
+    k_tgt_keys<<<grid_for(tcap, 256), 256, 0, st>>>(tcap, h.d_level_off, tv.coord, tv.parent, col, tv.child, tk, tb, dc); ++h.launches;
+    uint32_t *tk_s, *tb_s;
+    OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, tcap, 31, &tk_s, &tb_s));
+    h.tgt_key = tk_s;
+    h.tgt_box = tb_s;
+    const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
+    const int fill = h.tile_fill;   // targets per tile (the M2L batch width)
+    const int ntgt_bound = h.cap_mode ? tcap : std::max(0, nb - (h.max_level >= 2 ? h.level_off[2] : nb));
+    const int npad = ((ntgt_bound + fill - 1) / fill + 8) * tile;
+    int* gs;
+    uint32_t *pk, *pb;
+    OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
+    OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
+    OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
+    k_target_groups<<<1, 32, 0, st>>>(tk_s, dc, tile, fill, gs); ++h.launches;
+    k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, tile, fill, pk, pb); ++h.launches;
+    h.tgt_tile_key = pk;
+    h.tgt_tile_box = pb;
+    h.ntgt_pad = npad;
+    h.ntgt = ntgt_bound;
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }

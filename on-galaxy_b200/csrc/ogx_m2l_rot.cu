@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(RotCfg<P>::THREADS) k_m2l_rot(TreeView tv, con
     const int tid = threadIdx.x;
     const int ga = tid / R::ROWS, ra = tid % R::ROWS;   // block group; rows ra, ra + ROWS, ...
     const int base = blockIdx.x * ROT_TGT;
+    if (tv_over(tv)) return;
     if (tid == 0) s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
     __syncthreads();
     const int t = s_t;

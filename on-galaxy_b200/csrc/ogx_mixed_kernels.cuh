@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
     __shared__ int s_combo[189];      // present combinations: D | s << 5 | o << 8
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int base = blockIdx.x * 128;
+    if (tv_over(tv)) return;
     if (tid == 0) {
         s_t = (tgt_key[base] == 0xFFFFFFFFu) ? -1 : (int)tgt_key[base];
         s_abort = 0;
@@ -571,11 +572,12 @@ __global__ void __launch_bounds__(TcCfg<P>::THREADS, 1)
 // exactly when the M2L result is drained.
 template <int P>
 __global__ void __launch_bounds__(128) k_split_mpole(const double* __restrict__ M, int nb, __half* __restrict__ hi,
-                                                     __half* __restrict__ lo, float* __restrict__ munscale) {
+                                                     __half* __restrict__ lo, float* __restrict__ munscale,
+                                                     const DevCounts* counts) {
     using C = TcCfg<P>;
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (b >= nb) return;
+    if (b >= nb || b >= counts->nb32 || counts->overflow) return;
     const double* row = M + (size_t)b * C::K;
     double mx = 0.0;
     for (int k = lane; k < C::K; k += 32) mx = fmax(mx, fabs(row[k]));
@@ -599,7 +601,7 @@ __global__ void __launch_bounds__(128) k_m2l_dof0(TreeView tv, int ntgt_pad, con
                                                   const double* row0 /* 343 x K */, const double* M, double* lown) {
     constexpr int K = (P + 1) * (P + 1);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ntgt_pad || tgt_key[i] == 0xFFFFFFFFu) return;
+    if (i >= ntgt_pad || tv_over(tv) || tgt_key[i] == 0xFFFFFFFFu) return;
     const int b = (int)tgt_box[i], t = (int)tgt_key[i];
     const int par = tv.parent[b];
     const int tx = t & 1, ty = (t >> 1) & 1, tz = (t >> 2) & 1;
@@ -639,7 +641,7 @@ constexpr int NEAR_CAP = 128;    // source bodies staged per round (several U-li
 
 __global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restrict__ rhi, float4* __restrict__ rlo) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= tv.n) return;
+    if (i >= tv.n || tv_over(tv)) return;
     const double ex = tv.px[i] - tv.root->c[0], ey = tv.py[i] - tv.root->c[1], ez = tv.pz[i] - tv.root->c[2];
     const float hx = (float)ex, hy = (float)ey, hz = (float)ez;
     rhi[i] = make_float4(hx, hy, hz, (float)tv.pm[i]);
@@ -706,7 +708,9 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
     __shared__ float4 s_hi[NEAR_CAP], s_lo[NEAR_CAP];
     __shared__ double s_red[NU][4];
     const int lane = threadIdx.x & 31;
-    for (int lf = blockIdx.x; lf < tv.nleaf; lf += gridDim.x) {
+    if (tv_over(tv)) return;
+    const int nleaf = min(tv.nleaf, tv_nleaf(tv));
+    for (int lf = blockIdx.x; lf < nleaf; lf += gridDim.x) {
         const int b = tv.leafbox[lf];
         const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
         const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
@@ -825,9 +829,10 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
 // acc[orig] = G (far + near), pot[orig] = -G (far + near) (AdaptiveFMM3D.hpp:104)
 template <bool POT>
 __global__ void k_combine(int n, const int* __restrict__ perm, double G, const double* __restrict__ far,
-                          const double* __restrict__ near, double* __restrict__ acc, double* __restrict__ pot) {
+                          const double* __restrict__ near, double* __restrict__ acc, double* __restrict__ pot,
+                          const DevCounts* counts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || counts->overflow) return;
     const int o = perm[i];
     const double2 f0 = reinterpret_cast<const double2*>(far)[2 * (size_t)i];
     const double2 f1 = reinterpret_cast<const double2*>(far)[2 * (size_t)i + 1];
@@ -883,7 +888,7 @@ __global__ void __launch_bounds__(128) k_far_rec32(TreeView tv, int count, const
     constexpr int NE = MODE == 0 ? FarRec32<P>::NEH : FarRec32<P>::NEG;
     const int lane = threadIdx.x & 31;
     const int k = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (k >= count) return;
+    if (k >= count || k >= (MODE == 0 ? tv_nb(tv) : tv_nleaf(tv)) || tv_over(tv)) return;
     const int b = (MODE == 0) ? k : tv.leafbox[k];
     if (MODE == 0 && tv.x_off[b] == tv.x_off[b + 1]) return;   // never an M2P source
     const double* c = coef + (size_t)b * K;
@@ -1033,7 +1038,7 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(T
     __shared__ float4 s_res[FAR_WARPS][32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * FAR_WARPS + wid;
-    if (lf >= tv.nleaf) return;
+    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     const int64_t w0 = tv.w_off[lf];
@@ -1082,7 +1087,7 @@ constexpr size_t far_heavy_smem_bytes() { return FAR_HW * sizeof(float4) * (size
 // every leaf's result is computed independently); *count zero before the launch
 __global__ void k_far_heavy_list(TreeView tv, int* __restrict__ list, int* count) {
     const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lf >= tv.nleaf) return;
+    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
     if ((int64_t)tv.pcount[tv.leafbox[lf]] * (tv.w_off[lf + 1] - tv.w_off[lf]) > FAR_HEAVY) list[atomicAdd(count, 1)] = lf;
 }
 
@@ -1181,6 +1186,7 @@ __global__ void __launch_bounds__(32, 16) k_p2l32(TreeView tv, double* __restric
     __shared__ float s_red[32 * LD];
     const int lane = threadIdx.x;
     const int b = blockIdx.x;
+    if (b >= tv_nb(tv) || tv_over(tv)) return;
     const int64_t e0 = tv.x_off[b], e1 = tv.x_off[b + 1];
     if (e0 == e1) return;
     const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];

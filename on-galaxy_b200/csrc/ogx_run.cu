@@ -233,6 +233,7 @@ int ogx_ic_merger(void* handle, const ogx_merger_params* mp, int8_t* species_out
         return OGX_ERR_INVALID;
     Handle& h = *static_cast<Handle*>(handle);
     DevScope ds(h.device);
+    drop_step_graph(h);   // a new system: new sizes and capacities
     const int64_t np = mp->n_per, n = 2 * np;
     double *dp, *dv, *dm, *da, *dacc;
     int8_t* dsp;

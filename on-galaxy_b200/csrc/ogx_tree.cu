@@ -197,6 +197,8 @@ __global__ void k_counts_finalize(DevCounts* counts, const int64_t* recoff, cons
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     counts->num_boxes = recoff[n];
     counts->num_leaves = leafscan[n];
+    counts->nb32 = (int32_t)recoff[n];
+    counts->nleaf32 = (int32_t)leafscan[n];
     int run = 0, maxl = 0;
     int cum = 0;
     level_off_dev[0] = 0;
@@ -213,7 +215,8 @@ __global__ void k_counts_finalize(DevCounts* counts, const int64_t* recoff, cons
 
 __global__ void k_emit_records(const int* cnt, const int* dfirst, const int* leaflev, const int64_t* recoff, int64_t n,
                                uint32_t* reckey, uint32_t* recpos, const int* leafflag, const int64_t* leafscan,
-                               int* leafstart) {
+                               int* leafstart, const DevCounts* counts) {
+    if (counts->overflow) return;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i > n) return;
     if (i == n) { leafstart[leafscan[n]] = (int)n; return; }
@@ -230,12 +233,23 @@ __global__ void k_emit_records(const int* cnt, const int* dfirst, const int* lea
 }
 
 // ---- 4. boxes -------------------------------------------------------------------
-__global__ void k_boxes(int nb, const uint32_t* reclev, const uint32_t* recpos, const int* level_off, const uint64_t* khi,
+// k < nb_cap; records k >= the device box count are capacity padding: null boxes
+__global__ void k_boxes(int nb_cap, const uint32_t* reclev, const uint32_t* recpos, const int* level_off, const uint64_t* khi,
                         const uint32_t* klo, const int* leaflev, const int64_t* leafscan, const int* leafstart,
                         const RootInfo* root, int* level, int* coord, double* center, int* parent, int* child, int* leafid,
-                        int* pfirst, int* pcount, int* leafbox) {
+                        int* pfirst, int* pcount, int* leafbox, const DevCounts* counts) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nb) return;
+    if (k >= nb_cap || counts->overflow) return;
+    if (k >= counts->nb32) {
+        level[k] = -1;
+        coord[3 * k] = coord[3 * k + 1] = coord[3 * k + 2] = 0;
+        center[4 * k] = center[4 * k + 1] = center[4 * k + 2] = center[4 * k + 3] = 0.0;
+        parent[k] = -1;
+        leafid[k] = -1;
+        pfirst[k] = 0;
+        pcount[k] = 0;
+        return;
+    }
     const int l = (int)reclev[k];
     const int s = (int)recpos[k];
     const uint64_t hi = khi[s];
@@ -278,9 +292,10 @@ __global__ void k_boxes(int nb, const uint32_t* reclev, const uint32_t* recpos, 
     child[8 * lo_i + key_digit(hi, lo, l)] = k;
 }
 
-__global__ void k_leaf_occupancy(int nleaf, const int* leafbox, const int* pcount, DevCounts* counts) {
+__global__ void k_leaf_occupancy(int nleaf_cap, const int* leafbox, const int* pcount, DevCounts* counts) {
+    if (counts->overflow) return;
     const int lf = blockIdx.x * blockDim.x + threadIdx.x;
-    int c = (lf < nleaf) ? pcount[leafbox[lf]] : 0;
+    int c = (lf < nleaf_cap && lf < counts->nleaf32) ? pcount[leafbox[lf]] : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(FULL, c, o));
     if ((threadIdx.x & 31) == 0 && c > 0) atomicMax(&counts->max_leaf_occ, c);
@@ -306,11 +321,11 @@ __global__ void k_gather_bodies(const uint32_t* perm, const double* pos, const d
 }  // namespace
 
 static // flag the non-leaf boxes and count them per level
-__global__ void k_nonleaf_flags(int nb, const int* __restrict__ leafid, const int* __restrict__ level, int* flag,
+__global__ void k_nonleaf_flags(int nb_cap, const int* __restrict__ leafid, const int* __restrict__ level, int* flag,
                                 DevCounts* counts) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nb) return;
-    const int f = leafid[b] < 0;
+    if (b >= nb_cap) return;
+    const int f = !counts->overflow && b < counts->nb32 && leafid[b] < 0;
     flag[b] = f;
     if (f) atomicAdd(&counts->nonleaf_level[level[b]], 1);
 }
@@ -346,6 +361,21 @@ static inline int bits_for(int64_t v) {
     int b = 1;
     while ((1ll << b) <= v) ++b;
     return b;
+}
+
+// Capacity mode: flags an evaluation whose tree does not fit the capacities it was
+// launched with (or that needs the full 24-level key sort it was not launched with).
+__global__ void k_check_tree(DevCounts* counts, int nb_cap, int nleaf_cap, int levels_cap, int full_sort) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (counts->num_boxes > nb_cap || counts->num_leaves > nleaf_cap || counts->max_level + 1 > levels_cap ||
+        (counts->deep_flag && !full_sort))
+        counts->overflow = 1;
+}
+
+// a[k] = v for start <= k < cap, start read on the device (padding behind a device count)
+__global__ void k_fill_tail_u32(uint32_t* a, const int32_t* start, int64_t cap, uint32_t v) {
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (k < cap && k >= *start) a[k] = v;
 }
 
 int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) {
@@ -392,9 +422,13 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     // Leaves need the key order only down to their own level.  First attempt: sort
     // by levels 1..16 (6 of the 9 digit passes); if some level-16 box holds more than
     // thr bodies (deep clusters) the counts read at sync point 1 say so and the build
-    // is repeated with the full 72-bit sort.
+    // is repeated with the full 72-bit sort.  In capacity mode there is no read-back:
+    // the sort depth is the one the capacities were taken with, and a tree that needs
+    // more sets the overflow flag.
+    int nb = 0, nleaf = 0;
     for (int attempt = 0;; ++attempt) {
-        const int first_pass = (attempt == 0) ? 3 : 0;
+        const bool full = (attempt > 0) || (h.cap_mode && h.cap.full_sort);
+        const int first_pass = full ? 0 : 3;
         if (attempt > 0) OGX_CUDA(cudaMemsetAsync(dc, 0, sizeof(DevCounts), st));
         k_keys<<<grid_for(n, 256), 256, 0, st>>>(d_pos, n, root, khi_in, klo_in, kidx_in); ++h.launches;
         OGX_TRY(radix_sort_key72(h, n, first_pass, &khi, &klo, &kidx));
@@ -404,22 +438,40 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
         OGX_TRY(scan_i32_to_i64(h, cnt, recoff, n));
         OGX_TRY(scan_i32_to_i64(h, leafflag, leafscan, n));
         k_counts_finalize<<<1, 32, 0, st>>>(dc, recoff, leafscan, n, level_off_dev); ++h.launches;
+        if (h.cap_mode) {
+            nb = h.cap.nb;
+            nleaf = h.cap.nleaf;
+            k_check_tree<<<1, 32, 0, st>>>(dc, nb, nleaf, h.cap.levels, full ? 1 : 0); ++h.launches;
+            h.max_level = h.cap.levels - 1;
+            h.full_sort_used = full;
+            break;
+        }
         // sync point 1: box / leaf / level counts
         OGX_CUDA(cudaMemcpyAsync(h.h_counts, dc, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
         OGX_CUDA(cudaStreamSynchronize(st));
-        if (!h.h_counts->deep_flag || first_pass == 0) break;
+        if (!h.h_counts->deep_flag || first_pass == 0) {
+            h.full_sort_used = full;
+            break;
+        }
     }
-    const int nb = (int)h.h_counts->num_boxes;
-    const int nleaf = (int)h.h_counts->num_leaves;
-    h.max_level = h.h_counts->max_level;
-    h.level_off.assign(h.max_level + 2, 0);
-    for (int l = 0; l <= h.max_level; ++l) h.level_off[l + 1] = h.level_off[l] + h.h_counts->level_hist[l];
+    if (!h.cap_mode) {
+        nb = (int)h.h_counts->num_boxes;
+        nleaf = (int)h.h_counts->num_leaves;
+        h.max_level = h.h_counts->max_level;
+        h.level_off.assign(h.max_level + 2, 0);
+        for (int l = 0; l <= h.max_level; ++l) h.level_off[l + 1] = h.level_off[l] + h.h_counts->level_hist[l];
+    }
+    h.d_counts = dc;
+    h.d_level_off = level_off_dev;
 
+    // box records (level, first sorted body): capacity padding behind the device count
+    // gets level 31 and so sorts after every real record
     uint32_t *reckey, *recpos;
     OGX_TRY(arena_get(h.ws, S_REC_KEY, nb, &reckey));
     OGX_TRY(arena_get(h.ws, S_REC_POS, nb, &recpos));
     k_emit_records<<<grid_for(n + 1, 256), 256, 0, st>>>(cnt, dfirst, leaflev, recoff, n, reckey, recpos, leafflag, leafscan,
-                                                          leafstart); ++h.launches;
+                                                          leafstart, dc); ++h.launches;
+    if (h.cap_mode) { k_fill_tail_u32<<<grid_for(nb, 256), 256, 0, st>>>(reckey, &dc->nb32, nb, 31u); ++h.launches; }
     uint32_t *reclev, *recpos_s;
     OGX_TRY(radix_sort_u32(h, S_REC_KEY, S_REC_POS, S_REC_KEY2, S_REC_POS2, nb, 5, &reclev, &recpos_s));
 
@@ -437,7 +489,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_CUDA(cudaMemsetAsync(child, 0xFF, 8 * sizeof(int) * (size_t)nb, st));
     OGX_CUDA(cudaMemsetAsync(pcount, 0, sizeof(int) * (size_t)nb, st));
     k_boxes<<<grid_for(nb, 128), 128, 0, st>>>(nb, reclev, recpos_s, level_off_dev, khi, klo, leaflev, leafscan, leafstart, root,
-                                                level, coord, center, parent, child, leafid, pfirst, pcount, leafbox); ++h.launches;
+                                                level, coord, center, parent, child, leafid, pfirst, pcount, leafbox, dc); ++h.launches;
     k_leaf_occupancy<<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, leafbox, pcount, dc); ++h.launches;
 
     // non-leaf boxes in box order (level-major, so each level's parents are contiguous)
@@ -473,7 +525,7 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_CUDA(cudaGetLastError());
 
     TreeView& tv = h.tv;
-    tv.n = (int)n; tv.nb = nb; tv.nleaf = nleaf; tv.root = root;
+    tv.n = (int)n; tv.nb = nb; tv.nleaf = nleaf; tv.root = root; tv.cnt = dc;
     tv.px = px; tv.py = py; tv.pz = pz; tv.pm = pm; tv.perm = perm;
     tv.level = level; tv.coord = coord; tv.center = center; tv.parent = parent; tv.child = child;
     tv.leafid = leafid; tv.pfirst = pfirst; tv.pcount = pcount; tv.leafbox = leafbox;

@@ -49,14 +49,15 @@ class Stats(C.Structure):
                 ("adjacency_mismatch", C.c_int64),
                 ("ms_tree", C.c_double), ("ms_lists", C.c_double), ("ms_upward", C.c_double), ("ms_m2l", C.c_double),
                 ("ms_p2l", C.c_double), ("ms_downward", C.c_double), ("ms_leaf", C.c_double), ("ms_total", C.c_double),
-                ("ms_h2d", C.c_double), ("ms_d2h", C.c_double), ("launches", C.c_int64)]
+                ("ms_h2d", C.c_double), ("ms_d2h", C.c_double), ("launches", C.c_int64),
+                ("graph_steps", C.c_int64), ("step_redos", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Tuning(C.Structure):
-    _fields_ = [("m2l_tile_targets", C.c_int), ("near_units", C.c_int)]
+    _fields_ = [("m2l_tile_targets", C.c_int), ("near_units", C.c_int), ("capture_steps", C.c_int)]
 
 
 class MergerParams(C.Structure):
@@ -220,15 +221,18 @@ class _Solver:
     def synchronize(self):
         _check(self._lib.ogx_synchronize(self._h), "ogx_synchronize")
 
-    def set_tuning(self, m2l_tile_targets=0, near_units=0):
-        """Launch-shape knobs of the mixed form (0 keeps the default); see ogx_set_tuning."""
-        t = Tuning(int(m2l_tile_targets), int(near_units))
+    def set_tuning(self, m2l_tile_targets=0, near_units=0, capture_steps=None):
+        """Launch-shape knobs (0 keeps a size's default) and step capture (None keeps the
+        current setting); see ogx_set_tuning."""
+        if capture_steps is None:
+            capture_steps = self.tuning()["capture_steps"]
+        t = Tuning(int(m2l_tile_targets), int(near_units), int(bool(capture_steps)))
         _check(self._lib.ogx_set_tuning(self._h, C.byref(t)), "ogx_set_tuning")
 
     def tuning(self) -> dict:
         t = Tuning()
         _check(self._lib.ogx_get_tuning(self._h, C.byref(t)), "ogx_get_tuning")
-        return {"m2l_tile_targets": t.m2l_tile_targets, "near_units": t.near_units}
+        return {"m2l_tile_targets": t.m2l_tile_targets, "near_units": t.near_units, "capture_steps": t.capture_steps}
 
     def check_bounded_wait(self, polls=1000):
         """Run the pipeline's bounded device wait on a barrier nothing arrives on; raises
