@@ -97,6 +97,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-capture", action="store_true", help="eager steps instead of replaying a captured CUDA graph")
+    ap.add_argument("--no-serving", action="store_true", help="skip the ensemble (config 4) and serving (config 5) records")
     return ap.parse_args()
 
 
@@ -168,6 +169,53 @@ def cpu_baseline_single():
     return {"value": pos.shape[0] / sec, "unit": "bodies/s", "cores": 1, "kind": kind,
             "sample": f"one AdaptiveFMM3D evaluation of a {pos.shape[0]}-body merger (2x{pos.shape[0] // 2}, same "
                       f"generator), p={P_ORDER}, thr={THR}, {sec:.1f} s on 1 core; box has {os.cpu_count()} cores"}
+
+
+# ---------------------------------------------------------------- configs 4 and 5
+SERVE = os.path.join(PKG, "ogx_serve")
+CONFIG4 = ["--ensemble", "--steps", "20", "--jobs", "64", "--nmin", "8192", "--nmax", "262144", "--orders", "6,8",
+           "--seed", "3"]
+CONFIG5 = ["--jobs", "24", "--rate", "20", "--nmin", "16384", "--nmax", "1048576", "--orders", "6,8,12", "--smin", "10",
+           "--smax", "200", "--hbm-gb", "150", "--seed", "1"]
+
+
+def serve_run(args, timeout=600):
+    r = subprocess.run([SERVE, *args], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        return {"failed": r.returncode, "tail": (r.stdout + r.stderr)[-300:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    d.pop("jobs_detail", None)
+    return d
+
+
+def serving_records():
+    """Config 4 (64 resident systems, N log-uniform 8k-256k, p in {6, 8}, 20 lockstep steps)
+    and config 5 (24 jobs arriving at 20/s, N 16k-1M, p in {6, 8, 12}, 10-200 steps, 150 GB
+    budget) through the serving driver, mixed form, eager steps (a job's first steps would pay
+    for capturing its step, which these short jobs do not amortise);
+    config 4 also with every lockstep step as one graph launch, config 5 also as the plain
+    FP64 form run one job after another (the comparison config 5 names).  Seeded synthetic
+    jobs; wall-clock figures from the driver's own clock."""
+    out = {}
+    keep4 = ("bodies_steps_per_s", "ensemble_step_ms_p50", "ensemble_step_ms_p99", "p50_step_ms", "p99_step_ms",
+             "jobs", "failed", "rejected", "graph_launch_steps", "wall_s")
+    keep5 = ("bodies_steps_per_s", "stepping_only_bodies_steps_per_s", "p50_step_ms", "p99_step_ms",
+             "job_turnaround_s_p50", "job_turnaround_s_p99", "jobs", "failed", "rejected", "peak_concurrent", "wall_s")
+    try:
+        d = serve_run(CONFIG4)
+        out["config4_ensemble_workers"] = {k: d.get(k) for k in keep4} if "failed" not in d or d["failed"] == 0 else d
+        d = serve_run(CONFIG4 + ["--graph"])
+        out["config4_ensemble_one_launch_per_step"] = {k: d.get(k) for k in keep4} if "failed" not in d or d["failed"] == 0 else d
+        d = serve_run(CONFIG5)
+        out["config5_served_mixed"] = {k: d.get(k) for k in keep5} if "failed" not in d or d["failed"] == 0 else d
+        b = serve_run(CONFIG5 + ["--solo", "--precision", "fp64"], timeout=900)
+        out["config5_fp64_sequential"] = {k: b.get(k) for k in keep5} if "failed" not in b or b["failed"] == 0 else b
+        if d.get("bodies_steps_per_s") and b.get("bodies_steps_per_s"):
+            out["config5_served_over_fp64_sequential"] = d["bodies_steps_per_s"] / b["bodies_steps_per_s"]
+    except Exception as e:  # a failed record must not lose the headline line
+        out["error"] = repr(e)[:300]
+    out["note"] = "seeded synthetic jobs; bodies*steps/s over the driver's wall clock (set-up and arrivals included)"
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -407,6 +455,9 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_single()
+    if rank == 0 and world == 1 and not args.no_serving and os.path.exists(SERVE):
+        solver.close()
+        line["configs_4_5"] = serving_records()
     solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -177,6 +177,24 @@ int ogx_upload(void* handle, int64_t n, const double* pos, const double* vel, co
 int ogx_step(void* handle, double dt, int nsteps);
 int ogx_download(void* handle, double* pos, double* vel, double* acc);
 
+/* ---- ensembles: many resident systems advanced by one launch per step ----
+ * No counterpart in the reference (its integrator steps one system, Integrator3D.hpp:23-40).
+ * ogx_ensemble_create groups resident adaptive-FMM handles of one device (each keeps its own
+ * bodies, tree and expansions) and turns step capture on for them.  ogx_ensemble_step then
+ * takes `nsteps` leapfrog steps of every member: once every member has a captured step
+ * (see ogx_tuning.capture_steps; the first steps after creation or after a member's
+ * overflow are taken member by member), a step is one cudaGraphLaunch of a graph whose child
+ * graphs are the members' captured steps, so systems of any mix of N advance together with
+ * no host work between their kernels.  Each member's result equals its own eager steps.
+ * The members must not be used otherwise while an ensemble step runs.  ogx_ensemble_stats:
+ * out[0] steps taken by one launch, out[1] steps taken member by member, out[2] member steps
+ * redone after an overflow, out[3] times the ensemble graph was built.  Destroying the
+ * ensemble leaves the handles alive. */
+int ogx_ensemble_create(void* const* handles, int count, void** ensemble);
+int ogx_ensemble_step(void* ensemble, double dt, int nsteps);
+int ogx_ensemble_stats(void* ensemble, int64_t* out /* 4 */);
+int ogx_ensemble_destroy(void* ensemble);
+
 /* ---- tree export of the last adaptive evaluation (parity tests) ----
  * sizes[0]=boxes [1]=leaves [2..6]=|colleague|,|U|,|V|,|W|,|X| (AdaptiveOctree::buildLists,
  * src3d/AdaptiveOctree.hpp:137-189).

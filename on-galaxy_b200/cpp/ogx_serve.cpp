@@ -18,6 +18,12 @@
 // starts step s + 1), their steps spread over the same worker pool; the line then also
 // carries the lockstep step time (p50 / p99).
 //
+// --capture: every job's steps replay a CUDA graph of its step (ogx_tuning.capture_steps);
+// the results are bit-identical to eager steps.
+// --graph (with --ensemble): the systems advance through ogx_ensemble_step, every lockstep
+// step one CUDA graph launch whose child graphs are the systems' captured steps (the first
+// two steps are taken system by system while each captures its step).
+//
 // --autotune picks three knobs per job before it runs, by timing steps of dt = 0 of
 // that job alone (a coordinate search): the leaf capacity from {32, 48, 64, 96, 128}
 // (--thr fixes it instead, default 64), then the M2L batch width (targets per
@@ -138,6 +144,8 @@ double footprint_bytes(int64_t n, int p) {
     return 48e6 + 343.0 * K * K * 20.0 + (double)n * (1300.0 + 1.5 * K);
 }
 
+bool g_capture = false;   // --capture: every job replays its captured step (ogx_tuning.capture_steps)
+
 // create the job's handle and its initial conditions on the device
 void* open_job(Job& job, int precision) {
     ogx_params prm;
@@ -147,7 +155,7 @@ void* open_job(Job& job, int precision) {
     prm.precision = precision;
     void* h = nullptr;
     if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return nullptr;
-    ogx_tuning tu{job.fill, job.units};
+    ogx_tuning tu{job.fill, job.units, g_capture ? 1 : 0};
     if ((job.status = ogx_set_tuning(h, &tu)) != OGX_OK) {
         ogx_destroy(h);
         return nullptr;
@@ -368,7 +376,7 @@ int main(int argc, char** argv) {
     double rate = 20.0, hbm_gb = 150.0;
     int64_t nmin = 16384, nmax = 1 << 20;
     uint64_t seed = 1;
-    bool solo = false, ensemble = false, autotune = false;
+    bool solo = false, ensemble = false, autotune = false, graph = false;
     std::string tune_cache;
     int precision = OGX_PREC_MIXED, thr = 64, workers = 8;
     std::vector<int> orders = {6, 8, 12};
@@ -386,6 +394,8 @@ int main(int argc, char** argv) {
         else if (a == "--solo") solo = true;
         else if (a == "--ensemble") ensemble = true;
         else if (a == "--autotune") autotune = true;
+        else if (a == "--graph") graph = true;
+        else if (a == "--capture") g_capture = true;
         else if (a == "--tune-cache") tune_cache = next();
         else if (a == "--thr") thr = std::atoi(next().c_str());
         else if (a == "--workers") workers = std::atoi(next().c_str());
@@ -594,13 +604,42 @@ int main(int argc, char** argv) {
         round(T_OPEN);
         std::vector<float> ens_ms;
         const int S = smin;
+        int64_t gstats[4] = {0, 0, 0, 0};
+        void* ens = nullptr;
+        if (graph) {
+            std::vector<void*> hs;
+            for (Job* j : live)
+                if (j->h && j->status == OGX_OK) hs.push_back(j->h);
+            const int rc = hs.empty() ? OGX_ERR_STATE : ogx_ensemble_create(hs.data(), (int)hs.size(), &ens);
+            if (rc != OGX_OK) {
+                std::printf("{\"error\": \"ogx_ensemble_create: %s\"}\n", ogx_strerror(rc));
+                return 1;
+            }
+        }
         const auto e0 = std::chrono::steady_clock::now();
         for (int st = 0; st < S; ++st) {
             const auto t0 = std::chrono::steady_clock::now();
-            round(T_STEP);
+            if (graph) {
+                // every member's step in one launch (taken member by member until each
+                // member has a captured step)
+                const int rc = ogx_ensemble_step(ens, 0.01, 1);
+                const float ms = (float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                for (Job* j : live) {
+                    if (j->h && j->status == OGX_OK) {
+                        if (rc != OGX_OK) j->status = rc;
+                        else j->step_ms.push_back(ms);
+                    }
+                }
+            } else {
+                round(T_STEP);
+            }
             ens_ms.push_back((float)std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
         }
         const double ens_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - e0).count();
+        if (ens) {
+            ogx_ensemble_stats(ens, gstats);
+            ogx_ensemble_destroy(ens);
+        }
         lockstep = false;
         running = L;
         for (Job* j : live) push(j, T_CLOSE);
@@ -622,10 +661,12 @@ int main(int argc, char** argv) {
                     "\"steps\": %zu, \"lockstep_steps\": %d, \"workers\": %d, \"wall_s\": %.3f, \"bodies_steps_per_s\": %.6e, "
                     "\"ensemble_step_ms_p50\": %.3f, \"ensemble_step_ms_p99\": %.3f, \"p50_step_ms\": %.3f, "
                     "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"autotune\": %s, \"warmup_s\": %.3f, "
+                    "\"capture\": %s, \"graph\": %s, \"graph_launch_steps\": %lld, \"member_by_member_steps\": %lld, \"member_redos\": %lld, "
                     "\"jobs_detail\": [",
                     precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed", njobs, failed, rejected, all.size(), S, workers, ens_s,
                     bodysteps / ens_s, percentile(ens_ms, 0.5), percentile(ens_ms, 0.99), percentile(all, 0.5),
-                    percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s);
+                    percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s, g_capture ? "true" : "false", graph ? "true" : "false",
+                    (long long)gstats[0], (long long)gstats[1], (long long)gstats[2]);
         for (size_t j = 0; j < jobs.size(); ++j) {
             const Job& jb = jobs[j];
             std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, "
@@ -709,12 +750,13 @@ int main(int argc, char** argv) {
                 "\"steps\": %zu, \"workers\": %d, \"wall_s\": %.3f, \"warmup_s\": %.3f, \"bodies_steps_per_s\": %.6e, "
                 "\"stepping_only_bodies_steps_per_s\": %s, \"p50_step_ms\": %.3f, \"p99_step_ms\": %.3f, "
                 "\"job_turnaround_s_p50\": %s, \"job_turnaround_s_p99\": %s, "
-                "\"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"jobs_detail\": [",
+                "\"peak_concurrent\": %d, \"hbm_budget_gb\": %.1f, \"capture\": %s, \"jobs_detail\": [",
                 solo ? "solo" : "served", precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed", njobs, failed, rejected,
                 all.size(), solo ? 1 : workers, wall, warmup_s, bodysteps / wall,
                 solo ? std::to_string(step_s > 0 ? bodysteps / step_s : 0.0).c_str() : "null", percentile(all, 0.5),
                 percentile(all, 0.99), solo ? "null" : std::to_string(percentile(turnaround, 0.5)).c_str(),
-                solo ? "null" : std::to_string(percentile(turnaround, 0.99)).c_str(), solo ? 1 : peak, hbm_gb);
+                solo ? "null" : std::to_string(percentile(turnaround, 0.99)).c_str(), solo ? 1 : peak, hbm_gb,
+                g_capture ? "true" : "false");
     for (size_t j = 0; j < jobs.size(); ++j) {
         const Job& jb = jobs[j];
         std::printf("%s{\"id\": %d, \"n\": %lld, \"p\": %d, \"thr\": %d, \"m2l_tile_targets\": %d, \"near_units\": %d, "

@@ -167,9 +167,13 @@ static void update_capacity(Handle& h) {
     const DevCounts& c = *h.h_counts;
     Capacity& k = h.cap;
     const Capacity old = k;
-    k.nb = (int)(c.num_boxes + c.num_boxes / 8 + 256);
-    k.nleaf = (int)(c.num_leaves + c.num_leaves / 8 + 256);
+    k.nb = (int)(c.num_boxes + c.num_boxes / 8 + 128);
+    k.nleaf = (int)(c.num_leaves + c.num_leaves / 8 + 128);
     k.levels = std::min(kMaxDepth + 1, c.max_level + 2);
+    for (int l = 0; l < kMaxDepth + 2; ++l) {
+        const int b = (l <= c.max_level) ? c.level_hist[l] : (c.max_level >= 0 ? c.level_hist[c.max_level] : 0);
+        k.level_boxes[l] = b + b / 8 + 8;
+    }
     k.u = c.u_total + c.u_total / 8 + 4096;
     k.w = c.w_total + c.w_total / 8 + 4096;
     k.full_sort = h.full_sort_used;
@@ -328,7 +332,9 @@ static int capture_step(Handle& h, double* dp, double* dv, const double* dm, dou
         set_last_error(OGX_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ec));
         return OGX_ERR_CUDA;
     }
-    const cudaError_t ei = cudaGraphInstantiate(&h.step_exec, g, 0);
+    // node priorities as captured: the near field keeps the low priority of its stream, so
+    // it fills what the main chain leaves idle, as in an eager step
+    const cudaError_t ei = cudaGraphInstantiateWithFlags(&h.step_exec, g, cudaGraphInstantiateFlagUseNodePriority);
     if (ei != cudaSuccess) {
         cudaGraphDestroy(g);
         h.step_exec = nullptr;
@@ -338,6 +344,169 @@ static int capture_step(Handle& h, double* dp, double* dv, const double* dm, dou
     h.step_graph = g;
     h.step_launches = h.launches - l0;
     h.step_gen = h.ws.generation;
+    return OGX_OK;
+}
+
+// One step of a resident system (VelocityVerlet3D::step): eager, or with step capture
+// on (ogx_set_tuning) the first step after the capacities were set runs uncaptured in
+// capacity mode (every buffer grows to its capacity there), the next one is recorded as
+// a graph and later steps replay it.  Each step of a capturing handle copies its counts
+// to the host; a step whose tree or lists overflowed did nothing after its drift and is
+// redone eagerly here, which also sets new capacities.
+static int redo_overflowed(Handle& h, double dt) {
+    const int64_t n = h.n, n3 = 3 * n;
+    double *dp, *dv, *dm, *da, *dn;
+    OGX_TRY(arena_get(h.ws, S_POS, n3, &dp));
+    OGX_TRY(arena_get(h.ws, S_VEL, n3, &dv));
+    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
+    OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
+    OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
+    drop_step_graph(h);
+    h.cap_mode = false;
+    const int grid = (int)((n3 + 255) / 256);
+    OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
+    k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt, nullptr); ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    ++h.overflow_redos;
+    h.stats.launches += 1;
+    return OGX_OK;
+}
+
+int step_member(Handle& h, double dt) {
+    const int64_t n = h.n, n3 = 3 * n;
+    double *dp, *dv, *dm, *da, *dn;
+    OGX_TRY(arena_get(h.ws, S_POS, n3, &dp));
+    OGX_TRY(arena_get(h.ws, S_VEL, n3, &dv));
+    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
+    OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
+    OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
+    const bool graphed = h.capture_steps && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
+    if (!graphed) {
+        h.cap_mode = false;
+        OGX_TRY(step_once(h, dp, dv, dm, da, dn, dt));
+        h.stats.launches += 2;  // drift + kick around the evaluation
+        return OGX_OK;
+    }
+    if (h.step_exec && h.step_gen != h.ws.generation) drop_step_graph(h);
+    int64_t launched = 0;
+    if (h.step_exec) {
+        OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
+        h.launches += h.step_launches;
+        launched = h.step_launches;
+        ++h.graph_steps;
+    } else if (h.cap_warm == 0) {
+        const int64_t l0 = h.launches;
+        h.cap_mode = true;
+        const int rc = step_once(h, dp, dv, dm, da, dn, dt);
+        h.cap_mode = false;
+        OGX_TRY(rc);
+        h.cap_warm = 1;
+        launched = h.launches - l0;
+    } else {
+        OGX_TRY(capture_step(h, dp, dv, dm, da, dn, dt));
+        OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
+        launched = h.step_launches;
+        ++h.graph_steps;
+    }
+    OGX_CUDA(cudaStreamSynchronize(h.stream));
+    OGX_TRY(device_error(h));
+    if (h.h_counts->overflow) {
+        OGX_TRY(redo_overflowed(h, dt));
+    } else {
+        finish_stats(h);   // times and counts of the step that just ran
+        h.stats.launches = launched;
+    }
+    return OGX_OK;
+}
+
+// Members of an ensemble advance together: one CUDA graph whose child graphs are the
+// members' captured steps, launched once per ensemble step.
+struct Ensemble {
+    std::vector<Handle*> members;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraphExec_t> built_from;   // each member's step graph when `exec` was built
+    int64_t graph_steps = 0;    // ensemble steps taken by one launch of `exec`
+    int64_t member_steps = 0;   // ensemble steps taken member by member (warm-up, capture)
+    int64_t redos = 0;          // member steps redone eagerly after an overflow
+    int64_t rebuilds = 0;       // times `exec` was built
+};
+
+void drop_ensemble_graph(Ensemble& e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+    e.exec = nullptr;
+    e.graph = nullptr;
+    e.built_from.clear();
+}
+
+static bool ensemble_current(const Ensemble& e) {
+    if (!e.exec) return false;
+    for (size_t i = 0; i < e.members.size(); ++i) {
+        const Handle& h = *e.members[i];
+        if (!h.step_exec || h.step_exec != e.built_from[i] || h.step_gen != h.ws.generation) return false;
+    }
+    return true;
+}
+
+static int build_ensemble_graph(Ensemble& e) {
+    drop_ensemble_graph(e);
+    cudaGraph_t g = nullptr;
+    OGX_CUDA(cudaGraphCreate(&g, 0));
+    for (Handle* h : e.members) {
+        cudaGraphNode_t node;
+        const cudaError_t ec = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, h->step_graph);
+        if (ec != cudaSuccess) {
+            cudaGraphDestroy(g);
+            set_last_error(OGX_ERR_CUDA, std::string("cudaGraphAddChildGraphNode: ") + cudaGetErrorString(ec));
+            return OGX_ERR_CUDA;
+        }
+        e.built_from.push_back(h->step_exec);
+    }
+    const cudaError_t ei = cudaGraphInstantiateWithFlags(&e.exec, g, cudaGraphInstantiateFlagUseNodePriority);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        e.exec = nullptr;
+        e.built_from.clear();
+        set_last_error(OGX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+        return OGX_ERR_CUDA;
+    }
+    e.graph = g;
+    ++e.rebuilds;
+    return OGX_OK;
+}
+
+// One step of every member.  While some member has no current step graph (its first
+// steps, or after an overflow) the members step one by one; otherwise one launch runs
+// all of them, then each member's counts are checked and an overflowed member's step
+// is redone eagerly (so the ensemble graph is rebuilt at the next step).
+int ensemble_step(Ensemble& e, double dt) {
+    if (!ensemble_current(e)) {
+        drop_ensemble_graph(e);
+        for (Handle* h : e.members) OGX_TRY(step_member(*h, dt));
+        ++e.member_steps;
+        bool ready = true;
+        for (Handle* h : e.members) ready = ready && h->step_exec && h->step_gen == h->ws.generation;
+        if (ready) OGX_TRY(build_ensemble_graph(e));
+        return OGX_OK;
+    }
+    OGX_CUDA(cudaGraphLaunch(e.exec, e.stream));
+    OGX_CUDA(cudaStreamSynchronize(e.stream));
+    ++e.graph_steps;
+    for (Handle* h : e.members) {
+        h->launches += h->step_launches;
+        ++h->graph_steps;
+        OGX_TRY(device_error(*h));
+        if (h->h_counts->overflow) {
+            OGX_TRY(redo_overflowed(*h, dt));
+            ++e.redos;
+        } else {
+            finish_stats(*h);
+            h->stats.launches = h->step_launches;
+        }
+    }
+    for (Handle* h : e.members) OGX_CUDA(cudaStreamSynchronize(h->stream));
     return OGX_OK;
 }
 
@@ -548,65 +717,60 @@ int ogx_step(void* handle, double dt, int nsteps) {
     HANDLE(handle);
     if (!h.resident) return OGX_ERR_STATE;
     DeviceGuard g(h.device);
-    const int64_t n = h.n, n3 = 3 * n;
-    double *dp, *dv, *dm, *da, *dn;
-    OGX_TRY(arena_get(h.ws, S_POS, n3, &dp));
-    OGX_TRY(arena_get(h.ws, S_VEL, n3, &dv));
-    OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
-    OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
-    OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
-    for (int s = 0; s < nsteps; ++s) {
-        const bool graphed = h.capture_steps && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
-        if (!graphed) {
-            h.cap_mode = false;
-            OGX_TRY(step_once(h, dp, dv, dm, da, dn, dt));
-            h.stats.launches += 2;  // drift + kick around the evaluation
-            continue;
-        }
-        // Step capture: the first step after the capacities were set runs uncaptured
-        // in capacity mode (every buffer grows to its capacity there), the next one is
-        // recorded as a graph, and later steps replay it.  Each step copies its counts
-        // to the host; a step whose tree or lists overflowed did nothing after its
-        // drift and is redone eagerly here, which also sets new capacities.
-        if (h.step_exec && h.step_gen != h.ws.generation) drop_step_graph(h);
-        int64_t launched = 0;
-        if (h.step_exec) {
-            OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
-            h.launches += h.step_launches;
-            launched = h.step_launches;
-            ++h.graph_steps;
-        } else if (h.cap_warm == 0) {
-            const int64_t l0 = h.launches;
-            h.cap_mode = true;
-            const int rc = step_once(h, dp, dv, dm, da, dn, dt);
-            h.cap_mode = false;
-            OGX_TRY(rc);
-            h.cap_warm = 1;
-            launched = h.launches - l0;
-        } else {
-            OGX_TRY(capture_step(h, dp, dv, dm, da, dn, dt));
-            OGX_CUDA(cudaGraphLaunch(h.step_exec, h.stream));
-            launched = h.step_launches;
-            ++h.graph_steps;
-        }
-        OGX_CUDA(cudaStreamSynchronize(h.stream));
-        OGX_TRY(device_error(h));
-        if (h.h_counts->overflow) {
-            drop_step_graph(h);
-            h.cap_mode = false;
-            const int grid = (int)((n3 + 255) / 256);
-            OGX_TRY(eval_device(h, n, dp, dm, dn, nullptr));
-            k_kick<<<grid, 256, 0, h.stream>>>(dv, da, dn, n3, 0.5 * dt, nullptr); ++h.launches;
-            OGX_CUDA(cudaGetLastError());
-            ++h.overflow_redos;
-            h.stats.launches += 1;
-        } else {
-            finish_stats(h);   // times and counts of the step that just ran
-            h.stats.launches = launched;
-        }
-    }
+    for (int s = 0; s < nsteps; ++s) OGX_TRY(step_member(h, dt));
     OGX_CUDA(cudaGetLastError());
-    h.n = n;
+    return OGX_OK;
+}
+
+// ---- ensembles: every member's step in one graph launch --------------------------------
+int ogx_ensemble_create(void* const* handles, int count, void** out) {
+    if (!handles || count < 1 || !out) return OGX_ERR_INVALID;
+    *out = nullptr;
+    std::unique_ptr<Ensemble> e(new Ensemble);
+    for (int i = 0; i < count; ++i) {
+        if (!handles[i]) return OGX_ERR_INVALID;
+        Handle* h = static_cast<Handle*>(handles[i]);
+        if (!h->resident || h->prm.solver != OGX_SOLVER_ADAPTIVE_FMM) return OGX_ERR_STATE;
+        if (i > 0 && h->device != e->members[0]->device) return OGX_ERR_INVALID;
+        for (Handle* o : e->members)
+            if (o == h) return OGX_ERR_INVALID;
+        e->members.push_back(h);
+    }
+    DeviceGuard g(e->members[0]->device);
+    OGX_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    for (Handle* h : e->members) h->capture_steps = true;
+    *out = e.release();
+    return OGX_OK;
+}
+
+int ogx_ensemble_step(void* ens, double dt, int nsteps) {
+    if (!ens || nsteps < 0 || !std::isfinite(dt)) return OGX_ERR_INVALID;
+    Ensemble& e = *static_cast<Ensemble*>(ens);
+    DeviceGuard g(e.members[0]->device);
+    for (int s = 0; s < nsteps; ++s) OGX_TRY(ensemble_step(e, dt));
+    return OGX_OK;
+}
+
+int ogx_ensemble_stats(void* ens, int64_t* out) {
+    if (!ens || !out) return OGX_ERR_INVALID;
+    const Ensemble& e = *static_cast<const Ensemble*>(ens);
+    out[0] = e.graph_steps;
+    out[1] = e.member_steps;
+    out[2] = e.redos;
+    out[3] = e.rebuilds;
+    return OGX_OK;
+}
+
+int ogx_ensemble_destroy(void* ens) {
+    if (!ens) return OGX_ERR_INVALID;
+    Ensemble* e = static_cast<Ensemble*>(ens);
+    {
+        DeviceGuard g(e->members[0]->device);
+        if (e->stream) cudaStreamSynchronize(e->stream);
+        drop_ensemble_graph(*e);
+        if (e->stream) cudaStreamDestroy(e->stream);
+    }
+    delete e;
     return OGX_OK;
 }
 

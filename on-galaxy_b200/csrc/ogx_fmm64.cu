@@ -190,11 +190,12 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
     }
 }
 
-// CTAs of one level's translation: enough for the level's boxes (eager: the level
-// size is known on the host), or a fixed grid that walks the level (capacity mode)
+// CTAs of one level's translation: enough for the level's boxes (eager: the level size
+// is known on the host; capacity mode: the level's capacity; the CTAs walk the level's
+// parents in turn, so any count is covered)
 template <int P>
 int translate_grid(const Handle& h, int l) {
-    if (h.cap_mode) return 2 * h.num_sms;
+    if (h.cap_mode) return std::max(1, (h.cap.level_boxes[l] + tr_pb<P>() - 1) / tr_pb<P>());
     const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
     return (nbl + tr_pb<P>() - 1) / tr_pb<P>();
 }

@@ -199,6 +199,7 @@ __device__ __forceinline__ bool tv_over(const TreeView& tv) { return tv.cnt->ove
 struct Capacity {
     int nb = 0, nleaf = 0;
     int levels = 0;          // tree levels 0 .. levels-1 are walked by the translations
+    int level_boxes[kMaxDepth + 2] = {};   // boxes per level (sizes the translations' grids)
     int64_t u = 0, w = 0;    // U- and W-list entries
     bool full_sort = false;  // sort all 24 key levels (the tree had a deep cluster)
     bool valid = false;

@@ -33,6 +33,7 @@ EXPORTS = (
     "ogx_upload", "ogx_step", "ogx_download", "ogx_tree_sizes", "ogx_tree_boxes", "ogx_tree_list",
     "ogx_direct_eval_noalloc", "ogx_merger_params_default", "ogx_ic_merger", "ogx_set_species",
     "ogx_diagnostics", "ogx_download_frame", "ogx_check_bounded_wait", "ogx_set_tuning", "ogx_get_tuning",
+    "ogx_ensemble_create", "ogx_ensemble_step", "ogx_ensemble_stats", "ogx_ensemble_destroy",
 )
 
 

@@ -110,6 +110,20 @@ def test_ensemble_members_match_their_solo_runs():
 
 
 @pytest.mark.gpu
+def test_ensemble_in_one_graph_launch_per_step_matches_solo_runs():
+    """--graph: after each system has captured its step, a lockstep step of all systems is
+    one CUDA graph launch (ogx_ensemble_step); every system still ends bit-identical to its
+    solo run."""
+    args = ("--ensemble", "--steps", 6, "--jobs", 10, "--nmin", 8192, "--nmax", 131072, "--orders", "6,8",
+            "--seed", 5)
+    ens = _serve(*args, "--graph")
+    solo = _serve(*args, "--solo")
+    assert ens["graph"] is True and ens["failed"] == 0
+    assert ens["graph_launch_steps"] >= 2 and ens["graph_launch_steps"] + ens["member_by_member_steps"] == 6
+    assert [j["digest"] for j in ens["jobs_detail"]] == [j["digest"] for j in solo["jobs_detail"]]
+
+
+@pytest.mark.gpu
 def test_ensemble_autotune_picks_candidates_and_reuses_its_cache(tmp_path):
     """The tuner picks leaf capacity, M2L batch width and P2P tile shape from their candidate
     sets; its JSON cache is written after the run and, read by a second run, gives the same
