@@ -46,10 +46,10 @@ DT = 0.01
 
 # DRAM bytes per V-list pair of the tensor-core M2L launch: dram__bytes_read.sum +
 # dram__bytes_write.sum of one k_m2l_tc<8> launch on the merger with 2 x 250,000 bodies
-# (ncu --set full --clock-control none), (50.96 + 2.90) MB over its 3.42e6 V-list pairs.
+# (ncu --set full --clock-control none), (50.97 + 3.18) MB over its 3.42e6 V-list pairs.
 # The bytes scale with the pairs a launch processes (sources gathered per pair, results
 # per target), so the figure is applied to the measured workload's pair count.
-M2L_DRAM_BYTES_PER_VPAIR = 15.74
+M2L_DRAM_BYTES_PER_VPAIR = 15.82
 
 
 def arm_config(n, n_per, world):

@@ -937,9 +937,9 @@ constexpr int FAR_HEAVY = 1024;
 constexpr int FAR_HW = 8;
 
 // end of the M2P round that starts at task b0: at most 32 tasks spanning at most
-// FAR_R W boxes
-__device__ __forceinline__ int far_round_end(int b0, int nbk, int total) {
-    return min(total, min(b0 + 32, (b0 / nbk + FAR_R) * nbk));
+// R W boxes (the records one warp stages)
+__device__ __forceinline__ int far_round_end(int b0, int nbk, int total, int R) {
+    return min(total, min(b0 + 32, (b0 / nbk + R) * nbk));
 }
 
 // L2P of body block (nbk bodies staged in sx/sy/sz relative to the leaf centre):
@@ -1029,7 +1029,7 @@ __device__ __forceinline__ void far_m2p_round(const TreeView& tv, const float4* 
 // time (far_m2p_round), so a leaf of 17 bodies and 9 W boxes keeps every lane
 // busy.  Leaves with more than FAR_HEAVY tasks are left to k_leaf_far32_heavy.
 template <int P, bool POT>
-__global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
+__global__ void __launch_bounds__(32 * FAR_WARPS, 32 / FAR_WARPS) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
                                                                              const float4* __restrict__ grec,
                                                                              double* __restrict__ far) {
     constexpr int NEG = FarRec32<P>::NEG;
@@ -1064,7 +1064,7 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(T
         far_l2p<P>(g, nbk, sx, sy, sz, inv, srec, lane, acc);
         const int total = nbk * nw;
         for (int b0 = 0; b0 < total;) {
-            const int end = far_round_end(b0, nbk, total);
+            const int end = far_round_end(b0, nbk, total, FAR_R);
             far_m2p_round<P, POT>(tv, hrec, w0, nbk, b0, end, sx, sy, sz, cx, cy, cz, srec, s_res[wid], lane, acc);
             b0 = end;
         }
@@ -1080,8 +1080,13 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 24 / FAR_WARPS) k_leaf_far32(T
     }
 }
 
+// Heavy leaves have many bodies, so a round of 32 tasks rarely spans more than two W
+// boxes: two records per warp halve the CTA's shared memory (three CTAs per SM fit)
+constexpr int FAR_RH = 2;
 template <int P>
-constexpr size_t far_heavy_smem_bytes() { return FAR_HW * sizeof(float4) * (size_t)far_warp_f4<P>(); }
+constexpr int far_heavy_warp_f4() { return FAR_RH * 2 * FarRec32<P>::NEH; }
+template <int P>
+constexpr size_t far_heavy_smem_bytes() { return FAR_HW * sizeof(float4) * (size_t)far_heavy_warp_f4<P>(); }
 
 // list of the leaves with more than FAR_HEAVY M2P tasks (order irrelevant:
 // every leaf's result is computed independently); *count zero before the launch
@@ -1107,7 +1112,7 @@ __global__ void __launch_bounds__(32 * FAR_HW, 3) k_leaf_far32_heavy(TreeView tv
     __shared__ double s_part[FAR_HW][64][4];
     __shared__ int s_lf;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
+    float4* srec = s_far_dyn + (size_t)wid * far_heavy_warp_f4<P>();
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1138,7 +1143,7 @@ __global__ void __launch_bounds__(32 * FAR_HW, 3) k_leaf_far32_heavy(TreeView tv
             const int total = nbk * nw;
             int r = 0;
             for (int b0 = 0; b0 < total; ++r) {
-                const int end = far_round_end(b0, nbk, total);
+                const int end = far_round_end(b0, nbk, total, FAR_RH);
                 if (r % FAR_HW == wid)
                     far_m2p_round<P, POT>(tv, hrec, w0, nbk, b0, end, s_pos[0], s_pos[1], s_pos[2], cx, cy, cz, srec,
                                           s_res[wid], lane, acc);
