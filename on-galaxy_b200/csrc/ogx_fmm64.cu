@@ -50,17 +50,16 @@ int launch_far(Handle& h, const double* M, const double* L, double* far, bool po
     return OGX_OK;
 }
 
-// mixed form: FP32 records with folded weights, flat (body, W box) M2P tasks
+// mixed form: FP32 records with folded weights, flat (body, W box) M2P tasks.  The M2P
+// part needs only the multipoles, so it runs on the side stream beside the M2L and the
+// downward pass (into far_m); the L2P part runs after the downward pass (into far).
 template <int P>
-int launch_far32(Handle& h, const double* M, const double* L, double* far, bool pot) {
+int launch_far32_m2p(Handle& h, const double* M, double* far_m, bool pot, cudaStream_t st) {
     using R = mixed::FarRec32<P>;
-    const cudaStream_t st = h.stream;
     TreeView& tv = h.tv;
-    float4 *hrec, *grec;
+    float4* hrec;
     OGX_TRY(arena_get(h.ws, S_EVAL_H, (size_t)tv.nb * 2 * R::NEH, &hrec));
-    OGX_TRY(arena_get(h.ws, S_EVAL_G, (size_t)tv.nleaf * 2 * R::NEG, &grec));
     mixed::k_far_rec32<P, 0><<<(tv.nb + 3) / 4, 128, 0, st>>>(tv, tv.nb, M, hrec); ++h.launches;
-    mixed::k_far_rec32<P, 1><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, tv.nleaf, L, grec); ++h.launches;
     // heavy leaves: list, then one CTA of FAR_HW warps per leaf
     int* heavy;
     OGX_TRY(arena_get(h.ws, S_FAR_HEAVY, (size_t)tv.nleaf + 2, &heavy));
@@ -70,17 +69,28 @@ int launch_far32(Handle& h, const double* M, const double* L, double* far, bool 
     const size_t hsmem = mixed::far_heavy_smem_bytes<P>();
     const size_t smem = mixed::far_smem_bytes<P>();
     const int lgrid = (tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, lblock = 32 * mixed::FAR_WARPS;
-    if (pot) {
-        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32_heavy<P, true>, (int)hsmem));
-        mixed::k_leaf_far32_heavy<P, true><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
-        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32<P, true>, (int)smem));
-        mixed::k_leaf_far32<P, true><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
-    } else {
-        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32_heavy<P, false>, (int)hsmem));
-        mixed::k_leaf_far32_heavy<P, false><<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, grec, far, heavy, ctr); ++h.launches;
-        OGX_CUDA(smem_optin((const void*)mixed::k_leaf_far32<P, false>, (int)smem));
-        mixed::k_leaf_far32<P, false><<<lgrid, lblock, smem, st>>>(tv, hrec, grec, far); ++h.launches;
-    }
+    auto heavyk = pot ? mixed::k_leaf_far32_heavy<P, true, false> : mixed::k_leaf_far32_heavy<P, false, false>;
+    auto lightk = pot ? mixed::k_leaf_far32<P, true, false, true> : mixed::k_leaf_far32<P, false, false, true>;
+    OGX_CUDA(smem_optin((const void*)heavyk, (int)hsmem));
+    OGX_CUDA(smem_optin((const void*)lightk, (int)smem));
+    heavyk<<<2 * h.num_sms, 32 * mixed::FAR_HW, hsmem, st>>>(tv, hrec, nullptr, far_m, heavy, ctr); ++h.launches;
+    lightk<<<lgrid, lblock, smem, st>>>(tv, hrec, nullptr, far_m); ++h.launches;
+    return OGX_OK;
+}
+
+template <int P>
+int launch_far32_l2p(Handle& h, const double* L, double* far, bool pot) {
+    using R = mixed::FarRec32<P>;
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    float4* grec;
+    OGX_TRY(arena_get(h.ws, S_EVAL_G, (size_t)tv.nleaf * 2 * R::NEG, &grec));
+    mixed::k_far_rec32<P, 1><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, tv.nleaf, L, grec); ++h.launches;
+    const size_t smem = mixed::far_smem_bytes<P>();
+    const int lgrid = (tv.nleaf + mixed::FAR_WARPS - 1) / mixed::FAR_WARPS, lblock = 32 * mixed::FAR_WARPS;
+    auto l2pk = pot ? mixed::k_leaf_far32<P, true, true, false> : mixed::k_leaf_far32<P, false, true, false>;
+    OGX_CUDA(smem_optin((const void*)l2pk, (int)smem));
+    l2pk<<<lgrid, lblock, smem, st>>>(tv, nullptr, grec, far); ++h.launches;
     return OGX_OK;
 }
 
@@ -537,8 +547,9 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
     OGX_TRY(arena_get(h.ws, S_MIX_MUNSCALE, (size_t)tv.nb, &mus));
-    double* nearb;
+    double *nearb, *far_m;
     OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
+    OGX_TRY(arena_get(h.ws, S_FAR_M, 4 * (size_t)tv.n, &far_m));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
     // join the upward pass
@@ -573,6 +584,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         float4* rel;
         OGX_TRY(arena_get(h.ws, S_MIX_POS4, 2 * (size_t)tv.n, &rel));
         OGX_CUDA(cudaStreamWaitEvent(h.side, h.ev_fork, 0));
+        // the far field's M2P part (multipoles only) first, then the near field
+        OGX_TRY(launch_far32_m2p<P>(h, M, far_m, d_pot != nullptr, h.side));
         mixed::k_near_prep<<<(tv.n + 255) / 256, 256, 0, h.side>>>(tv, rel, rel + tv.n); ++h.launches;
         const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
         auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32> : mixed::k_leaf_near32<true, 64>)
@@ -587,12 +600,12 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(launch_l2l<P>(h, L, Lown));
     OGX_CUDA(timing_record(h, h.ev[6], st));
     const bool pot = d_pot != nullptr;
-    OGX_TRY(launch_far32<P>(h, M, L, far, pot));
-    // join the near field, then acc = G (far + near) in the caller's order
+    OGX_TRY(launch_far32_l2p<P>(h, L, far, pot));
+    // join the side stream (M2P, near field), then acc = G (far + near) in the caller's order
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_join, 0));
     const double G = h.prm.G;
-    if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, d_pot, tv.cnt); ++h.launches; }
-    else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, nearb, d_acc, nullptr, tv.cnt); ++h.launches; }
+    if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, far_m, nearb, d_acc, d_pot, tv.cnt); ++h.launches; }
+    else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, far_m, nearb, d_acc, nullptr, tv.cnt); ++h.launches; }
     OGX_CUDA(timing_record(h, h.ev[7], st));
     OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaGetLastError());

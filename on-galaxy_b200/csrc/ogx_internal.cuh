@@ -74,7 +74,7 @@ enum Slot {
     S_U_CNT, S_W_CNT, S_U_OFF, S_W_OFF, S_U_IDX, S_W_IDX,
     S_X_KEY, S_X_VAL, S_X_KEY2, S_X_VAL2, S_X_OFF, S_X_IDX, S_X_CNT, S_PERM_FINAL,
     S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, S_TGT_TILE, S_TGT_PKEY, S_TGT_PBOX,
-    S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_NEAR, S_SCAN_TMP,
+    S_MPOLE, S_LOCAL, S_LOWN, S_FAR, S_FAR_M, S_NEAR, S_SCAN_TMP,
     S_OPS_M2L, S_OPS_M2M, S_OPS_L2L,
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_MUNSCALE, S_MIX_OUNSCALE, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,

@@ -827,15 +827,21 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
 }
 
 // acc[orig] = G (far + near), pot[orig] = -G (far + near) (AdaptiveFMM3D.hpp:104)
+// far = far_l (L2P) + far_m (M2P) when the two parts ran apart (far_m non-null)
 template <bool POT>
 __global__ void k_combine(int n, const int* __restrict__ perm, double G, const double* __restrict__ far,
-                          const double* __restrict__ near, double* __restrict__ acc, double* __restrict__ pot,
-                          const DevCounts* counts) {
+                          const double* __restrict__ far_m, const double* __restrict__ near, double* __restrict__ acc,
+                          double* __restrict__ pot, const DevCounts* counts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || counts->overflow) return;
     const int o = perm[i];
-    const double2 f0 = reinterpret_cast<const double2*>(far)[2 * (size_t)i];
-    const double2 f1 = reinterpret_cast<const double2*>(far)[2 * (size_t)i + 1];
+    double2 f0 = reinterpret_cast<const double2*>(far)[2 * (size_t)i];
+    double2 f1 = reinterpret_cast<const double2*>(far)[2 * (size_t)i + 1];
+    if (far_m) {
+        const double2 m0 = reinterpret_cast<const double2*>(far_m)[2 * (size_t)i];
+        const double2 m1 = reinterpret_cast<const double2*>(far_m)[2 * (size_t)i + 1];
+        f0.x += m0.x; f0.y += m0.y; f1.x += m1.x; f1.y += m1.y;
+    }
     const double2 n0 = reinterpret_cast<const double2*>(near)[2 * (size_t)i];
     const double2 n1 = reinterpret_cast<const double2*>(near)[2 * (size_t)i + 1];
     acc[3 * (size_t)o] = G * (f0.x + n0.x);
@@ -1027,8 +1033,10 @@ __device__ __forceinline__ void far_m2p_round(const TreeView& tv, const float4* 
 // centre staged in FP64 shared memory.  L2P: lanes over bodies.  M2P: the
 // (body, W box) pairs of the block form a flat W-major task list taken 32 at a
 // time (far_m2p_round), so a leaf of 17 bodies and 9 W boxes keeps every lane
-// busy.  Leaves with more than FAR_HEAVY tasks are left to k_leaf_far32_heavy.
-template <int P, bool POT>
+// busy.  The mixed form runs the two parts apart: M2P (DO_M2P, multipoles only) beside
+// the M2L and the downward pass, L2P (DO_L2P) after the downward pass.  With DO_M2P,
+// leaves with more than FAR_HEAVY tasks are left to k_leaf_far32_heavy.
+template <int P, bool POT, bool DO_L2P, bool DO_M2P>
 __global__ void __launch_bounds__(32 * FAR_WARPS, 32 / FAR_WARPS) k_leaf_far32(TreeView tv, const float4* __restrict__ hrec,
                                                                              const float4* __restrict__ grec,
                                                                              double* __restrict__ far) {
@@ -1042,12 +1050,12 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 32 / FAR_WARPS) k_leaf_far32(T
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     const int64_t w0 = tv.w_off[lf];
-    const int nw = (int)(tv.w_off[lf + 1] - w0);
-    if ((int64_t)cnt * nw > FAR_HEAVY) return;
+    const int nw = DO_M2P ? (int)(tv.w_off[lf + 1] - w0) : 0;
+    if (DO_M2P && (int64_t)cnt * nw > FAR_HEAVY) return;
     float4* srec = s_far_dyn + (size_t)wid * far_warp_f4<P>();
     const double cx = tv.center[4 * b], cy = tv.center[4 * b + 1], cz = tv.center[4 * b + 2];
     const double inv = 1.0 / (2.0 * tv.center[4 * b + 3]);
-    const float4* g = grec + (size_t)lf * 2 * NEG;
+    const float4* g = DO_L2P ? grec + (size_t)lf * 2 * NEG : nullptr;
     double* sx = s_pos[wid][0];
     double* sy = s_pos[wid][1];
     double* sz = s_pos[wid][2];
@@ -1061,7 +1069,7 @@ __global__ void __launch_bounds__(32 * FAR_WARPS, 32 / FAR_WARPS) k_leaf_far32(T
             sz[j] = tv.pz[i] - cz;
         }
         double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-        far_l2p<P>(g, nbk, sx, sy, sz, inv, srec, lane, acc);
+        if (DO_L2P) far_l2p<P>(g, nbk, sx, sy, sz, inv, srec, lane, acc);
         const int total = nbk * nw;
         for (int b0 = 0; b0 < total;) {
             const int end = far_round_end(b0, nbk, total, FAR_R);
@@ -1101,7 +1109,7 @@ __global__ void k_far_heavy_list(TreeView tv, int* __restrict__ list, int* count
 // before the launch; ctr[0] = list length) so the CTAs balance themselves.  Warp w runs the M2P rounds r = w, w + FAR_HW, ...;
 // warp 0 also the L2P; the warps' per-body partial sums are added in warp order
 // through shared memory (deterministic).
-template <int P, bool POT>
+template <int P, bool POT, bool DO_L2P>
 __global__ void __launch_bounds__(32 * FAR_HW, 3) k_leaf_far32_heavy(TreeView tv, const float4* __restrict__ hrec,
                                                                  const float4* __restrict__ grec, double* __restrict__ far,
                                                                  const int* __restrict__ list, int* ctr) {
@@ -1139,7 +1147,7 @@ __global__ void __launch_bounds__(32 * FAR_HW, 3) k_leaf_far32_heavy(TreeView tv
             }
             __syncthreads();
             double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-            if (wid == 0) far_l2p<P>(grec + (size_t)lf * 2 * NEG, nbk, s_pos[0], s_pos[1], s_pos[2], inv, srec, lane, acc);
+            if (DO_L2P && wid == 0) far_l2p<P>(grec + (size_t)lf * 2 * NEG, nbk, s_pos[0], s_pos[1], s_pos[2], inv, srec, lane, acc);
             const int total = nbk * nw;
             int r = 0;
             for (int b0 = 0; b0 < total; ++r) {
