@@ -144,6 +144,8 @@ const char* ogx_strerror(int status);
  *                      the capacities does nothing after its drift and is redone eagerly
  *                      inside the same ogx_step call (new capacities, new capture), so the
  *                      results are those of eager steps.  Each step ends with a host sync.
+ *                      A handle whose stream is the legacy or per-thread default stream
+ *                      steps eagerly (capture is not possible there).
  * ogx_set_tuning applies from the next evaluation on; 0 in a size field keeps its default. */
 typedef struct {
     int m2l_tile_targets;
@@ -186,7 +188,8 @@ int ogx_download(void* handle, double* pos, double* vel, double* acc);
  * overflow are taken member by member), a step is one cudaGraphLaunch of a graph whose child
  * graphs are the members' captured steps, so systems of any mix of N advance together with
  * no host work between their kernels.  Each member's result equals its own eager steps.
- * The members must not be used otherwise while an ensemble step runs.  ogx_ensemble_stats:
+ * The members must not be used otherwise while an ensemble step runs, and they must outlive
+ * the ensemble; they keep step capture on after it is destroyed.  ogx_ensemble_stats:
  * out[0] steps taken by one launch, out[1] steps taken member by member, out[2] member steps
  * redone after an overflow, out[3] times the ensemble graph was built.  Destroying the
  * ensemble leaves the handles alive. */

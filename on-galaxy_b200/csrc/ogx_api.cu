@@ -380,7 +380,10 @@ int step_member(Handle& h, double dt) {
     OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
     OGX_TRY(arena_get(h.ws, S_ACC, n3, &da));
     OGX_TRY(arena_get(h.ws, S_ACC_OLD, n3, &dn));
-    const bool graphed = h.capture_steps && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
+    // a step on the legacy or per-thread default stream cannot be captured: such a handle
+    // steps eagerly
+    const bool capturable = h.stream != nullptr && h.stream != cudaStreamLegacy && h.stream != cudaStreamPerThread;
+    const bool graphed = h.capture_steps && capturable && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
     if (!graphed) {
         h.cap_mode = false;
         OGX_TRY(step_once(h, dp, dv, dm, da, dn, dt));
