@@ -591,6 +591,9 @@ int ogx_create(const ogx_params* prm, void** handle) {
     OGX_CUDA(cudaStreamCreateWithPriority(&h->main, cudaStreamNonBlocking, prio_high));
     OGX_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_low));
     OGX_CUDA(cudaStreamCreateWithPriority(&h->up, cudaStreamNonBlocking, prio_high));
+    OGX_CUDA(cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_high));
+    OGX_CUDA(cudaEventCreateWithFlags(&h->ev_col, cudaEventDisableTiming));
+    OGX_CUDA(cudaEventCreateWithFlags(&h->ev_tgt, cudaEventDisableTiming));
     for (cudaEvent_t* e : {&h->ev_fork, &h->ev_join, &h->ev_in, &h->ev_out, &h->ev_tree, &h->ev_up})
         OGX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreate(&h->ev_up_end));
@@ -611,7 +614,9 @@ int ogx_destroy(void* handle) {
         if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto& e : h->ev)
             if (e) cudaEventDestroy(e);
-        for (cudaStream_t sx : {h->main, h->side, h->up})
+        for (cudaEvent_t e : {h->ev_col, h->ev_tgt})
+            if (e) cudaEventDestroy(e);
+        for (cudaStream_t sx : {h->main, h->side, h->up, h->aux})
             if (sx) {
                 cudaStreamSynchronize(sx);
                 cudaStreamDestroy(sx);

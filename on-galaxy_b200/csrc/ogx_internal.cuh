@@ -235,6 +235,8 @@ struct Handle {
     // from and joined back to the caller's stream; overlapping work goes to `side`
     // (lowest priority) so it only fills SMs the main chain leaves idle
     cudaStream_t main = nullptr, side = nullptr, up = nullptr;
+    cudaStream_t aux = nullptr;                  // M2L target tiles, beside the U/W list passes
+    cudaEvent_t ev_col = nullptr, ev_tgt = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_in = nullptr, ev_out = nullptr, ev_tree = nullptr, ev_up = nullptr;
     cudaEvent_t ev_up_end = nullptr;   // timing: end of an upward pass that ran on `up`
     bool upward_split = false;         // the last evaluation ran its upward pass on `up`

@@ -363,6 +363,42 @@ int lists_build(Handle& h) {
     k_colleagues_check<<<grid_for(nb, 4), 128, 0, st>>>(0, nb, tv.leafid, tv.child, tv.center, tv.root, col, dc); ++h.launches;
     tv.col = col;
 
+    // M2L targets (levels >= 2) grouped by child octant, then by the slot pattern of
+    // their V lists; launched over the box capacity, the padding sorts last.  They need
+    // only the colleagues, so they are built on the aux stream beside the U/W passes
+    // (which use the scan scratch, not the radix-sort scratch); the main stream joins
+    // before the X-list sort, which uses the radix-sort scratch again.
+    OGX_CUDA(cudaEventRecord(h.ev_col, st));
+    OGX_CUDA(cudaStreamWaitEvent(h.aux, h.ev_col, 0));
+    h.stream = h.aux;   // radix_sort_u32 issues on h.stream
+    const int tcap = std::max(nb, 1);
+    uint32_t *tk, *tb;
+    OGX_TRY(arena_get(h.ws, S_TGT_KEY, tcap + 1, &tk));
+    OGX_TRY(arena_get(h.ws, S_TGT_BOX, tcap + 1, &tb));
+    k_tgt_keys<<<grid_for(tcap, 256), 256, 0, h.aux>>>(tcap, h.d_level_off, tv.coord, tv.parent, col, tv.child, tk, tb, dc); ++h.launches;
+    uint32_t *tk_s, *tb_s;
+    const int rc_t = radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, tcap, 31, &tk_s, &tb_s);
+    h.stream = st;
+    OGX_TRY(rc_t);
+    h.tgt_key = tk_s;
+    h.tgt_box = tb_s;
+    const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
+    const int fill = h.tile_fill;   // targets per tile (the M2L batch width)
+    const int ntgt_bound = h.cap_mode ? tcap : std::max(0, nb - (h.max_level >= 2 ? h.level_off[2] : nb));
+    const int npad = ((ntgt_bound + fill - 1) / fill + 8) * tile;
+    int* gs;
+    uint32_t *pk, *pb;
+    OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
+    OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
+    OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
+    k_target_groups<<<1, 32, 0, h.aux>>>(tk_s, dc, tile, fill, gs); ++h.launches;
+    k_target_pad<<<grid_for(npad, 256), 256, 0, h.aux>>>(tb_s, gs, npad, tile, fill, pk, pb); ++h.launches;
+    h.tgt_tile_key = pk;
+    h.tgt_tile_box = pb;
+    h.ntgt_pad = npad;
+    h.ntgt = ntgt_bound;
+    OGX_CUDA(cudaEventRecord(h.ev_tgt, h.aux));
+
     int *ucnt, *wcnt, *lane_uw;
     int64_t *uoff, *woff;
     OGX_TRY(arena_get(h.ws, S_U_CNT, nleaf, &ucnt));
@@ -402,6 +438,7 @@ int lists_build(Handle& h) {
                                                         widx, dc); ++h.launches;
     tv.u_off = uoff; tv.w_off = woff; tv.u_idx = uidx; tv.w_idx = widx;
 
+    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_tgt, 0));   // target sort done with the radix scratch
     // X lists: W transposed by a stable sort on the W member; keys behind the W total
     // (capacity padding) sort last and are never referenced by x_off
     const int xbits = bits_for(nb);
@@ -421,32 +458,6 @@ int lists_build(Handle& h) {
     tv.x_off = xoff;
     tv.x_idx = (const int*)xv_s;
 
-    // M2L targets (levels >= 2) grouped by child octant, then by the slot pattern of
-    // their V lists; launched over the box capacity, the padding sorts last
-    const int tcap = std::max(nb, 1);
-    uint32_t *tk, *tb;
-    OGX_TRY(arena_get(h.ws, S_TGT_KEY, tcap + 1, &tk));
-    OGX_TRY(arena_get(h.ws, S_TGT_BOX, tcap + 1, &tb));
-    k_tgt_keys<<<grid_for(tcap, 256), 256, 0, st>>>(tcap, h.d_level_off, tv.coord, tv.parent, col, tv.child, tk, tb, dc); ++h.launches;
-    uint32_t *tk_s, *tb_s;
-    OGX_TRY(radix_sort_u32(h, S_TGT_KEY, S_TGT_BOX, S_TGT_KEY2, S_TGT_BOX2, tcap, 31, &tk_s, &tb_s));
-    h.tgt_key = tk_s;
-    h.tgt_box = tb_s;
-    const int tile = 128;  // tensor-core M2L tile; a multiple of the FP64 kernel's 64
-    const int fill = h.tile_fill;   // targets per tile (the M2L batch width)
-    const int ntgt_bound = h.cap_mode ? tcap : std::max(0, nb - (h.max_level >= 2 ? h.level_off[2] : nb));
-    const int npad = ((ntgt_bound + fill - 1) / fill + 8) * tile;
-    int* gs;
-    uint32_t *pk, *pb;
-    OGX_TRY(arena_get(h.ws, S_TGT_TILE, 32, &gs));
-    OGX_TRY(arena_get(h.ws, S_TGT_PKEY, npad, &pk));
-    OGX_TRY(arena_get(h.ws, S_TGT_PBOX, npad, &pb));
-    k_target_groups<<<1, 32, 0, st>>>(tk_s, dc, tile, fill, gs); ++h.launches;
-    k_target_pad<<<grid_for(npad, 256), 256, 0, st>>>(tb_s, gs, npad, tile, fill, pk, pb); ++h.launches;
-    h.tgt_tile_key = pk;
-    h.tgt_tile_box = pb;
-    h.ntgt_pad = npad;
-    h.ntgt = ntgt_bound;
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
