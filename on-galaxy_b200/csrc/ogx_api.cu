@@ -228,8 +228,10 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     if (!h.cap_mode) update_capacity(h);
     if (h.prm.precision == OGX_PREC_MIXED) OGX_TRY(fmm_mixed(h, d_acc, d_pot));
     else OGX_TRY(fmm_fp64(h, d_acc, d_pot));   // the plain form, or with rotation-based M2L
-    // every count of this evaluation (the overflow flag included) reaches the host with it
+    // every count of this evaluation (the overflow flag included) reaches the host with it,
+    // and so does the error word of its bounded waits (tensor-core M2L, translation passes)
     OGX_CUDA(cudaMemcpyAsync(h.h_counts, h.d_counts, sizeof(DevCounts), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(timing_record(h, h.ev[8], st));
     h.stats.launches = h.launches - l0;
     return OGX_OK;
@@ -256,7 +258,7 @@ static void counts_to_stats(Handle& h) {
 static int device_error(Handle& h) {
     if (h.h_err && *h.h_err) {
         *h.h_err = 0;
-        set_last_error(OGX_ERR_TIMEOUT, "a bounded device wait ran out (mbarrier wait of the tensor-core M2L pipeline)");
+        set_last_error(OGX_ERR_TIMEOUT, "a bounded device wait ran out (tensor-core M2L pipeline or a translation pass)");
         return OGX_ERR_TIMEOUT;
     }
     return OGX_OK;

@@ -4,15 +4,16 @@
 // but organised for the GPU:
 //   P2M           warp per leaf: lanes build harmonics of 32 bodies into shared
 //                 memory, then reduce columns (:53-61, FmmExpansions3D.hpp:148-163)
-//   M2M           per level bottom-up, warp per parent, level-independent
-//                 matrices MM_s (:62-71)
+//   M2M           bottom-up in one launch (groups of parents taken level by level,
+//                 each waiting for its children), warp per child octant,
+//                 level-independent matrices MM_s (:62-71)
 //   M2L           all levels in one launch: targets grouped by their octant in
 //                 the parent, 64 per CTA; for each of the 189 (colleague slot,
 //                 child) combinations the sources of all 64 targets are gathered
 //                 into shared memory and multiplied by the offset's matrix T_o
 //                 (:78-81; V list implicit in the colleague slots)
 //   P2L           warp per box over its X list (:82, :117-128)
-//   L2L           per level top-down, warp per box (:75-77)
+//   L2L           top-down in one launch, the same way (:75-77)
 //   leaf far      warp per leaf: L2P through gradient coefficients of L, M2P
 //                 over the W list through gradient coefficients of M (:92-93)
 //   leaf near     warp per leaf: softened P2P over the U list, j != i (:95-103),
@@ -94,52 +95,114 @@ int launch_far32_l2p(Handle& h, const double* L, double* far, bool pot) {
     return OGX_OK;
 }
 
-// ---- M2M (MODE 0) / L2L (MODE 1) over the non-leaf parents of one level ------------
+// ---- M2M (MODE 0) / L2L (MODE 1): one launch per pass ---------------------------------
 // CTA = tr_pb<P>() parents x 8 warps, warp s = child octant s.  Warp s applies the
 // operator MM_s / LL_s (transposed, k-major, L2-resident) to its TR_PB parents,
 // lanes over output dofs.
 //   M2M: M'_P = sum_s MM_s M'_{child s}                (src3d/AdaptiveFMM3D.hpp:62-71)
 //        the eight partial products are summed in octant order through shared memory
 //   L2L: L'_{child s} = L'own_{child s} + LL_s L'_P     (src3d/AdaptiveFMM3D.hpp:75-77)
+// The reference walks the levels one after another (its GPU form launches once per
+// level, src3d/gpu/AdaptiveFMM3DGPU.cu:274-289).  Here one launch covers every level.
+// The CTAs take groups of TR_PB parents of one level by ticket (an atomic counter) in
+// level order: root level first for L2L, deepest level first for M2M.  A group waits
+// until its inputs are final: for L2L each parent's local, written by the group that
+// holds the parent's parent; for M2M each non-leaf child's multipole.  Those groups hold
+// earlier tickets, taken by CTAs that are already running, so every wait ends; each is
+// bounded all the same (one that runs out sets *err).  A group publishes its boxes with
+// a fence and a release store of ready[box]; data written in this launch is read
+// through L2 (ld.global.cg).  The arithmetic per box is the same in any order.
 // parents per CTA: each warp applies its operator to TR_PB parents per load of an
 // operator row (4 where the shared staging fits the 48 KB static limit)
 template <int P>
 constexpr int tr_pb() { return (P + 1) * (P + 1) <= 81 ? 4 : 2; }
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// bounded wait until *flag != 0; false when it ran out (*err is then set) or when
+// another wait already gave up
+__device__ bool wait_ready(const int* flag, int* err) {
+    for (uint32_t it = 0; it < sm100::kSpinLimit; ++it) {
+        if (ld_acquire_gpu(flag)) return true;
+        if (*(volatile int*)err) return false;
+        if (it > 16) __nanosleep(64);
+    }
+    atomicExch(err, 1);
+    return false;
+}
+
 template <int P, int MODE>
-__global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* __restrict__ nonleaf,
-                                                       const int* __restrict__ nl_off, int level,
-                                                       const double* __restrict__ opsT, double* mpole, double* local,
-                                                       const double* __restrict__ lown) {
+__global__ void __launch_bounds__(256) k_translate_flow(TreeView tv, const int* __restrict__ nonleaf,
+                                                        const int* __restrict__ nl_off, int nlev,
+                                                        const double* __restrict__ opsT, double* mpole, double* local,
+                                                        const double* __restrict__ lown, int* ready, int* ticket,
+                                                        int* err) {
     constexpr int K = (P + 1) * (P + 1);
     constexpr int NPL = (K + 31) / 32;
     constexpr int TR_PB = tr_pb<P>();
     __shared__ double s_in[MODE == 0 ? 8 : 1][TR_PB][K];
     __shared__ double s_part[MODE == 0 ? 8 : 1][TR_PB][MODE == 0 ? K : 1];
+    __shared__ int s_gend[kMaxDepth + 2];   // groups of the pass's first i+1 levels
+    __shared__ int s_t;
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
-    // this level's non-leaf parents (count known on the device only): the CTAs take
-    // groups of TR_PB parents in turn
-    if (tv_over(tv)) return;
-    const int first = nl_off[level], count = nl_off[level + 1] - first;
-    const int* parents = nonleaf + first;
-    for (int p0 = blockIdx.x * TR_PB; p0 < count; p0 += gridDim.x * TR_PB) {
-        if (MODE == 0) __syncthreads();   // s_part of the previous group is read
+    if (tv_over(tv) || nlev <= 0) return;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int i = 0; i < nlev; ++i) {
+            const int l = MODE == 1 ? i : nlev - 1 - i;
+            c += (nl_off[l + 1] - nl_off[l] + TR_PB - 1) / TR_PB;
+            s_gend[i] = c;
+        }
+    }
+    for (;;) {
+        __syncthreads();   // s_gend is written; the previous group's shared data was read
+        if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= s_gend[nlev - 1]) break;
+        int i = 0;
+        while (t >= s_gend[i]) ++i;
+        const int l = MODE == 1 ? i : nlev - 1 - i;
+        const int p0 = (t - (i > 0 ? s_gend[i - 1] : 0)) * TR_PB;
+        const int first = nl_off[l], count = nl_off[l + 1] - first;
         int bx[TR_PB], ch[TR_PB];
         bool any = false;
 #pragma unroll
         for (int a = 0; a < TR_PB; ++a) {
-            bx[a] = (p0 + a < count) ? parents[p0 + a] : -1;
+            bx[a] = (p0 + a < count) ? nonleaf[first + p0 + a] : -1;
             ch[a] = (bx[a] >= 0) ? tv.child[8 * bx[a] + s] : -1;
             any |= ch[a] >= 0;
         }
+        // wait for this group's inputs
+        if (MODE == 1) {
+            if (l > 0 && threadIdx.x < TR_PB) {
+                int b = -1;
+#pragma unroll
+                for (int a = 0; a < TR_PB; ++a) b = (a == (int)threadIdx.x) ? bx[a] : b;
+                if (b >= 0) wait_ready(ready + b, err);   // published by the group of b's parent
+            }
+        } else if (lane < TR_PB) {
+            int c = -1;
+#pragma unroll
+            for (int a = 0; a < TR_PB; ++a) c = (a == lane) ? ch[a] : c;
+            if (c >= 0 && tv.leafid[c] < 0) wait_ready(ready + c, err);
+        }
+        __syncthreads();
         if (MODE == 0) {
 #pragma unroll
             for (int a = 0; a < TR_PB; ++a)
-                for (int d = lane; d < K; d += 32) s_in[s][a][d] = (ch[a] >= 0) ? mpole[(size_t)ch[a] * K + d] : 0.0;
+                for (int d = lane; d < K; d += 32) s_in[s][a][d] = (ch[a] >= 0) ? __ldcg(mpole + (size_t)ch[a] * K + d) : 0.0;
             __syncwarp();
         } else {
 #pragma unroll
             for (int a = 0; a < TR_PB; ++a)
-                for (int d = threadIdx.x; d < K; d += blockDim.x) s_in[0][a][d] = (bx[a] >= 0) ? local[(size_t)bx[a] * K + d] : 0.0;
+                for (int d = threadIdx.x; d < K; d += blockDim.x) s_in[0][a][d] = (bx[a] >= 0) ? __ldcg(local + (size_t)bx[a] * K + d) : 0.0;
             __syncthreads();
         }
         double acc[TR_PB][NPL];
@@ -176,6 +239,14 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
                     if (j < K) local[(size_t)ch[a] * K + j] = lown[(size_t)ch[a] * K + j] + acc[a][q];
                 }
             }
+            __threadfence();
+            __syncthreads();
+            if (lane < TR_PB) {
+                int c = -1;
+#pragma unroll
+                for (int a = 0; a < TR_PB; ++a) c = (a == lane) ? ch[a] : c;
+                if (c >= 0) st_release_gpu(ready + c, 1);
+            }
         } else {
 #pragma unroll
             for (int a = 0; a < TR_PB; ++a)
@@ -195,28 +266,59 @@ __global__ void __launch_bounds__(256) k_translate_oct(TreeView tv, const int* _
                     mpole[(size_t)bx[a] * K + d] = v;
                 }
             }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x < TR_PB) {
+                int b = -1;
+#pragma unroll
+                for (int a = 0; a < TR_PB; ++a) b = (a == (int)threadIdx.x) ? bx[a] : b;
+                if (b >= 0) st_release_gpu(ready + b, 1);
+            }
         }
-        if (MODE == 1) __syncthreads();   // s_in is refilled for the next group
     }
 }
 
-// CTAs of one level's translation: enough for the level's boxes (eager: the level size
-// is known on the host; capacity mode: the level's capacity; the CTAs walk the level's
-// parents in turn, so any count is covered)
+// Groups of one level's translation: enough for the level's boxes (eager: the level
+// size is known on the host; capacity mode: the level's capacity)
 template <int P>
-int translate_grid(const Handle& h, int l) {
-    if (h.cap_mode) return std::max(1, (h.cap.level_boxes[l] + tr_pb<P>() - 1) / tr_pb<P>());
+int translate_groups(const Handle& h, int l) {
+    if (h.cap_mode) return (h.cap.level_boxes[l] + tr_pb<P>() - 1) / tr_pb<P>();
     const int nbl = h.level_off[l + 1] - h.level_off[l];   // bound on the level's parents
     return (nbl + tr_pb<P>() - 1) / tr_pb<P>();
 }
 
+// one launch of a translation pass: CTAs for every SM (as many as fit), at most one per
+// group; the ready flags and the ticket counter are cleared first
+template <int P, int MODE>
+int launch_translate(Handle& h, Slot slot, double* M, double* L, const double* Lown) {
+    const int nlev = h.max_level;   // parent levels 0 .. max_level-1
+    if (nlev <= 0) return OGX_OK;
+    int groups = 0;
+    for (int l = 0; l < nlev; ++l) groups += translate_groups<P>(h, l);
+    if (groups <= 0) return OGX_OK;
+    static const int per_sm = [] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_translate_flow<P, MODE>, 256, 0) != cudaSuccess) {
+            cudaGetLastError();
+            b = 1;
+        }
+        return std::max(1, b);
+    }();
+    int* ready;
+    OGX_TRY(arena_get(h.ws, slot, (size_t)h.tv.nb + 1, &ready));
+    OGX_CUDA(cudaMemsetAsync(ready, 0, sizeof(int) * ((size_t)h.tv.nb + 1), h.stream));
+    const int grid = std::min(groups, per_sm * h.num_sms);
+    k_translate_flow<P, MODE><<<grid, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, nlev,
+                                                          MODE == 0 ? h.d_m2m : h.d_l2l, M, L, Lown, ready,
+                                                          ready + h.tv.nb, h.d_err);
+    ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
 template <int P>
 int launch_m2m(Handle& h, double* M) {
-    for (int l = h.max_level - 1; l >= 0; --l) {
-        const int g = translate_grid<P>(h, l);
-        if (g > 0) { k_translate_oct<P, 0><<<g, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_m2m, M, nullptr, nullptr); ++h.launches; }
-    }
-    return OGX_OK;
+    return launch_translate<P, 0>(h, S_TR_READY_M, M, nullptr, nullptr);
 }
 
 template <int P>
@@ -224,11 +326,7 @@ int launch_l2l(Handle& h, double* L, const double* Lown) {
     constexpr int K = (P + 1) * (P + 1);
     // root (no parent): its local is its own M2L/P2L part
     OGX_CUDA(cudaMemcpyAsync(L, Lown, sizeof(double) * K, cudaMemcpyDeviceToDevice, h.stream));   // box 0 is the root
-    for (int l = 0; l < h.max_level; ++l) {
-        const int g = translate_grid<P>(h, l);
-        if (g > 0) { k_translate_oct<P, 1><<<g, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, l, h.d_l2l, nullptr, L, Lown); ++h.launches; }
-    }
-    return OGX_OK;
+    return launch_translate<P, 1>(h, S_TR_READY_L, nullptr, L, Lown);
 }
 
 // ---- M2L (structured, FP64) -----------------------------------------------------------
@@ -607,7 +705,6 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     if (pot) { mixed::k_combine<true><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, far_m, nearb, d_acc, d_pot, tv.cnt); ++h.launches; }
     else { mixed::k_combine<false><<<(tv.n + 255) / 256, 256, 0, st>>>(tv.n, tv.perm, G, far, far_m, nearb, d_acc, nullptr, tv.cnt); ++h.launches; }
     OGX_CUDA(timing_record(h, h.ev[7], st));
-    OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
