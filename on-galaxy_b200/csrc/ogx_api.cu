@@ -221,7 +221,11 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     // while the lists are built
     h.upward_split = (h.prm.precision == OGX_PREC_MIXED);
     if (h.upward_split) OGX_TRY(fmm_mixed_upward(h));
-    OGX_TRY(lists_build(h));
+    OGX_TRY(lists_build_targets(h));
+    // mixed form: the M2L needs the multipoles and the target tiles only, so it starts
+    // beside the U/W/X list build
+    if (h.prm.precision == OGX_PREC_MIXED) OGX_TRY(fmm_mixed_m2l(h, d_pot != nullptr));
+    OGX_TRY(lists_build_uwx(h));
     OGX_CUDA(timing_record(h, h.ev[9], st));
     h.tree_valid = true;
     // an eager evaluation has read its counts back by now: capacities for capacity mode
@@ -594,8 +598,13 @@ int ogx_create(const ogx_params* prm, void** handle) {
     OGX_CUDA(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_low));
     OGX_CUDA(cudaStreamCreateWithPriority(&h->up, cudaStreamNonBlocking, prio_high));
     OGX_CUDA(cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_high));
+    // the M2L between the list build (high) and the side stream (low), where the
+    // device has a level between them
+    const int prio_mid = (prio_high - prio_low <= -2 || prio_high - prio_low >= 2) ? (prio_low + prio_high) / 2 : prio_high;
+    OGX_CUDA(cudaStreamCreateWithPriority(&h->m2l, cudaStreamNonBlocking, prio_mid));
     OGX_CUDA(cudaEventCreateWithFlags(&h->ev_col, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreateWithFlags(&h->ev_tgt, cudaEventDisableTiming));
+    OGX_CUDA(cudaEventCreateWithFlags(&h->ev_m2l, cudaEventDisableTiming));
     for (cudaEvent_t* e : {&h->ev_fork, &h->ev_join, &h->ev_in, &h->ev_out, &h->ev_tree, &h->ev_up})
         OGX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreate(&h->ev_up_end));
@@ -616,9 +625,9 @@ int ogx_destroy(void* handle) {
         if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto& e : h->ev)
             if (e) cudaEventDestroy(e);
-        for (cudaEvent_t e : {h->ev_col, h->ev_tgt})
+        for (cudaEvent_t e : {h->ev_col, h->ev_tgt, h->ev_m2l})
             if (e) cudaEventDestroy(e);
-        for (cudaStream_t sx : {h->main, h->side, h->up, h->aux})
+        for (cudaStream_t sx : {h->main, h->side, h->up, h->aux, h->m2l})
             if (sx) {
                 cudaStreamSynchronize(sx);
                 cudaStreamDestroy(sx);

@@ -628,53 +628,72 @@ int run_mixed_upward(Handle& h) {
     return OGX_OK;
 }
 
+// Mixed-form M2L on the tensor cores, on h.m2l: it waits for the FP16 split of the
+// multipoles (h.ev_up) and the target tiles (h.ev_tgt) and runs beside the U/W/X list
+// build; run_mixed joins it (h.ev_m2l) before the P2L, which adds into the same locals.
 template <int P>
-int run_mixed(Handle& h, double* d_acc, double* d_pot) {
+int run_mixed_m2l(Handle& h, bool pot) {
     using C = mixed::TcCfg<P>;
     constexpr int K = (P + 1) * (P + 1);
     constexpr int LD = K | 1;
-    const cudaStream_t st = h.stream;
+    const cudaStream_t sm = h.m2l;
     TreeView& tv = h.tv;
-    double *M, *L, *Lown, *far;
+    double *M, *Lown;
     __half *mhi, *mlo;
     float* mus;
     OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
-    OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
     OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
-    OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
     OGX_TRY(arena_get(h.ws, S_MIX_MHI, (size_t)tv.nb * C::KPAD, &mhi));
     OGX_TRY(arena_get(h.ws, S_MIX_MLO, (size_t)tv.nb * C::KPAD, &mlo));
     OGX_TRY(arena_get(h.ws, S_MIX_MUNSCALE, (size_t)tv.nb, &mus));
-    double *nearb, *far_m;
-    OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
-    OGX_TRY(arena_get(h.ws, S_FAR_M, 4 * (size_t)tv.n, &far_m));
-    const size_t p2x_smem = p2x_smem_bytes<P, float>();
-    OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
-    // join the upward pass
-    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
-    OGX_CUDA(timing_record(h, h.ev[3], st));
-    // the near field needs only the tree and the lists: it may start with the M2L
-    OGX_CUDA(cudaEventRecord(h.ev_fork, st));
-    // M2L on the tensor cores
-    OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, st));
+    OGX_CUDA(cudaStreamWaitEvent(sm, h.ev_up, 0));
+    OGX_CUDA(cudaStreamWaitEvent(sm, h.ev_tgt, 0));
+    OGX_CUDA(timing_record(h, h.ev[3], sm));
+    OGX_CUDA(cudaMemsetAsync(Lown, 0, sizeof(double) * (size_t)tv.nb * K, sm));
     if (h.ntgt > 0) {
         if constexpr (C::SUPPORTED) {
             OGX_CUDA(smem_optin((const void*)mixed::k_m2l_tc<P>, C::SMEM));
-            mixed::k_m2l_tc<P><<<dim3(h.ntgt_pad / 128, C::NSPLIT), C::THREADS, C::SMEM, st>>>(
+            mixed::k_m2l_tc<P><<<dim3(h.ntgt_pad / 128, C::NSPLIT), C::THREADS, C::SMEM, sm>>>(
                 tv, h.tgt_tile_key, h.tgt_tile_box, mhi, mlo, mus, h.d_tc_img, h.d_tc_ounscale, Lown, h.d_err); ++h.launches;
-            if (d_pot) {
-                mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, st>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,
+            if (pot) {
+                mixed::k_m2l_dof0<P><<<(h.ntgt_pad + 127) / 128, 128, 0, sm>>>(tv, h.ntgt_pad, h.tgt_tile_key, h.tgt_tile_box,
                                                                              h.d_tc_row0, M, Lown); ++h.launches;
             }
         } else {
             // an order whose operand would not fit TMEM even in slices: the FP64 M2L serves it
             const size_t m2l_smem = (size_t)M2L_TGT * LD * sizeof(double);
             OGX_CUDA(smem_optin((const void*)k_m2l_fp64<P>, (int)m2l_smem));
-            k_m2l_fp64<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, m2l_smem, st>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M,
+            k_m2l_fp64<P><<<h.ntgt_pad / M2L_TGT, M2L_THREADS, m2l_smem, sm>>>(tv, h.tgt_tile_key, h.tgt_tile_box, h.d_m2l, M,
                                                                            Lown); ++h.launches;
         }
     }
-    // near field on the low-priority side stream, launched after the M2L (which takes
+    OGX_CUDA(timing_record(h, h.ev[4], sm));
+    OGX_CUDA(cudaEventRecord(h.ev_m2l, sm));
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+template <int P>
+int run_mixed(Handle& h, double* d_acc, double* d_pot) {
+    constexpr int K = (P + 1) * (P + 1);
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    double *M, *L, *Lown, *far;
+    OGX_TRY(arena_get(h.ws, S_MPOLE, (size_t)tv.nb * K, &M));
+    OGX_TRY(arena_get(h.ws, S_LOCAL, (size_t)tv.nb * K, &L));
+    OGX_TRY(arena_get(h.ws, S_LOWN, (size_t)tv.nb * K, &Lown));
+    OGX_TRY(arena_get(h.ws, S_FAR, 4 * (size_t)tv.n, &far));
+    double *nearb, *far_m;
+    OGX_TRY(arena_get(h.ws, S_NEAR32, 4 * (size_t)tv.n, &nearb));
+    OGX_TRY(arena_get(h.ws, S_FAR_M, 4 * (size_t)tv.n, &far_m));
+    const size_t p2x_smem = p2x_smem_bytes<P, float>();
+    OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
+    // join the upward pass (the side stream's M2P reads the multipoles)
+    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
+    // the far field's M2P part and the near field need the tree, the multipoles and the
+    // lists: they start here, beside the M2L (launched on h.m2l before the U/W/X lists)
+    OGX_CUDA(cudaEventRecord(h.ev_fork, st));
+    // near field on the low-priority side stream, issued after the M2L (which takes
     // whole SMs first): its one-warp blocks fill what the M2L's tiles leave free, the
     // SMs its last wave leaves idle, and then what P2L, L2L and the far field leave idle
     {
@@ -691,7 +710,8 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches;
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
-    OGX_CUDA(timing_record(h, h.ev[4], st));
+    // join the M2L (its end is timing event 4, recorded on h.m2l)
+    OGX_CUDA(cudaStreamWaitEvent(st, h.ev_m2l, 0));
     if constexpr (mixed::P2L32<P>::OK) { mixed::k_p2l32<P><<<tv.nb, 32, 0, st>>>(tv, Lown); ++h.launches; }
     else { k_p2x<P, 1, float><<<(tv.nb + 3) / 4, 128, p2x_smem, st>>>(tv, tv.nb, Lown); ++h.launches; }
     OGX_CUDA(timing_record(h, h.ev[5], st));
@@ -725,6 +745,24 @@ int fmm_mixed_upward(Handle& h) {
         case 10: return run_mixed_upward<10>(h);
         case 11: return run_mixed_upward<11>(h);
         case 12: return run_mixed_upward<12>(h);
+        default: return OGX_ERR_INVALID;
+    }
+}
+
+int fmm_mixed_m2l(Handle& h, bool pot) {
+    switch (h.prm.p) {
+        case 1: return run_mixed_m2l<1>(h, pot);
+        case 2: return run_mixed_m2l<2>(h, pot);
+        case 3: return run_mixed_m2l<3>(h, pot);
+        case 4: return run_mixed_m2l<4>(h, pot);
+        case 5: return run_mixed_m2l<5>(h, pot);
+        case 6: return run_mixed_m2l<6>(h, pot);
+        case 7: return run_mixed_m2l<7>(h, pot);
+        case 8: return run_mixed_m2l<8>(h, pot);
+        case 9: return run_mixed_m2l<9>(h, pot);
+        case 10: return run_mixed_m2l<10>(h, pot);
+        case 11: return run_mixed_m2l<11>(h, pot);
+        case 12: return run_mixed_m2l<12>(h, pot);
         default: return OGX_ERR_INVALID;
     }
 }

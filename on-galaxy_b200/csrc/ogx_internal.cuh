@@ -236,7 +236,10 @@ struct Handle {
     // (lowest priority) so it only fills SMs the main chain leaves idle
     cudaStream_t main = nullptr, side = nullptr, up = nullptr;
     cudaStream_t aux = nullptr;                  // M2L target tiles, beside the U/W list passes
-    cudaEvent_t ev_col = nullptr, ev_tgt = nullptr;
+    // mixed form: the tensor-core M2L (middle priority), launched once the multipoles and
+    // target tiles are ready, beside the rest of the list build
+    cudaStream_t m2l = nullptr;
+    cudaEvent_t ev_col = nullptr, ev_tgt = nullptr, ev_m2l = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_in = nullptr, ev_out = nullptr, ev_tree = nullptr, ev_up = nullptr;
     cudaEvent_t ev_up_end = nullptr;   // timing: end of an upward pass that ran on `up`
     bool upward_split = false;         // the last evaluation ran its upward pass on `up`
@@ -301,11 +304,14 @@ bool build_rot_pack(int p, int index, double* out /* rot_pack_size(p) */);
 
 // ---- phases (defined in the .cu files) -------------------------------------
 int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);
-int lists_build(Handle& h);
+int lists_build(Handle& h);           // both parts below, in order
+int lists_build_targets(Handle& h);   // colleagues; M2L target tiles on `aux`
+int lists_build_uwx(Handle& h);       // U, W and X lists
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int m2l_rot_launch(Handle& h, const double* M, double* Lown);   // third form's M2L, on h.stream
 int fmm_mixed_upward(Handle& h);   // upward pass on h.up, right after the tree (before the lists)
+int fmm_mixed_m2l(Handle& h, bool pot);   // tensor-core M2L on h.m2l, after the target tiles
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);

@@ -353,9 +353,14 @@ inline int bits_for(int64_t v) {
 }  // namespace
 
 int lists_build(Handle& h) {
+    OGX_TRY(lists_build_targets(h));
+    return lists_build_uwx(h);
+}
+
+int lists_build_targets(Handle& h) {
     const cudaStream_t st = h.stream;
     TreeView& tv = h.tv;
-    const int nb = tv.nb, nleaf = tv.nleaf;   // launch sizes (capacities in capacity mode)
+    const int nb = tv.nb;   // launch size (the capacity in capacity mode)
     DevCounts* dc = h.d_counts;
     int* col;
     OGX_TRY(arena_get(h.ws, S_BOX_COL, 27 * (size_t)nb, &col));
@@ -398,7 +403,16 @@ int lists_build(Handle& h) {
     h.ntgt_pad = npad;
     h.ntgt = ntgt_bound;
     OGX_CUDA(cudaEventRecord(h.ev_tgt, h.aux));
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
 
+int lists_build_uwx(Handle& h) {
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    const int nb = tv.nb, nleaf = tv.nleaf;   // launch sizes (capacities in capacity mode)
+    DevCounts* dc = h.d_counts;
+    const int* col = tv.col;
     int *ucnt, *wcnt, *lane_uw;
     int64_t *uoff, *woff;
     OGX_TRY(arena_get(h.ws, S_U_CNT, nleaf, &ucnt));
