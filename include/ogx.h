@@ -14,7 +14,8 @@
  *     no exit() across the ABI; ogx_strerror() names the code.
  *   - positions/accelerations: n x 3 doubles (x,y,z per body), original order.
  *   - potentials: n doubles, pot_i = -G * sum_{j!=i} m_j / sqrt(r_ij^2 + eps^2)
- *     (direct) or its FMM approximation; NULL skips the potential.
+ *     (direct) or its FMM approximation (the spline kernel's potential with
+ *     OGX_SOFT_SPLINE); NULL skips the potential.
  *   - a handle is not thread-safe: one handle per host thread / stream.
  *   - all device work is issued on the handle's stream.
  */
@@ -53,15 +54,32 @@ typedef enum {
                            * order (README.md:75 of the reference defers this operator) */
 } ogx_precision;
 
+/* Softening kernel.  The reference softens with Plummer's kernel in the P2P part only and
+ * evaluates the far field unsoftened (src3d/AdaptiveFMM3D.hpp:18, :97-105), so every pair the
+ * expansions take at a distance comparable to eps sees a different force than it would in the
+ * near field; its README names that seam as the cause of its energy drift (README.md:73-75).
+ * OGX_SOFT_SPLINE, beyond the reference: the cubic-spline kernel of Monaghan & Lattanzio (1985)
+ * in the form GADGET-2 uses (Springel 2005), with support h = 2.8 eps (the potential at r = 0
+ * equals Plummer's, -G m / eps).  It is exactly Newtonian for r >= h, so the unsoftened
+ * expansions are exact for it there; every pair closer than h that the far field takes (leaves
+ * that are not adjacent but lie within h of each other) is corrected by a direct pass with the
+ * difference of the two kernels.  The result is the spline-softened force up to the truncation
+ * error of the expansions, with no seam.  Steps of such a handle are never captured. */
+typedef enum {
+    OGX_SOFT_PLUMMER = 0, /* the reference's kernel: m / (r^2 + eps^2)^{3/2} (Kernel3D.hpp:24-42) */
+    OGX_SOFT_SPLINE = 1   /* compact cubic spline, h = 2.8 eps, with the far field corrected within h */
+} ogx_softening;
+
 typedef struct {
     double G;            /* gravitational constant (KernelParams3D::G) */
-    double eps;          /* Plummer softening (KernelParams3D::eps); also the leaf-edge floor */
+    double eps;          /* softening length (KernelParams3D::eps); also the leaf-edge floor */
     int p;               /* expansion order, 1..12 (AdaptiveFMM3D p) */
     int leaf_capacity;   /* split threshold (AdaptiveFMM3D threshold), >= 1 */
     int solver;          /* ogx_solver */
     int precision;       /* ogx_precision */
     int device;          /* CUDA device ordinal */
     void* stream;        /* cudaStream_t to issue on; NULL = a stream owned by the handle */
+    int softening;       /* an ogx_softening value; default OGX_SOFT_PLUMMER, the reference's kernel */
 } ogx_params;
 
 typedef struct {
@@ -80,9 +98,11 @@ typedef struct {
     int64_t launches;          /* kernels launched by the last evaluation (+ drift/kick in ogx_step) */
     int64_t graph_steps;       /* ogx_step calls' steps replayed from a captured graph (running total) */
     int64_t step_redos;        /* steps redone eagerly after a capacity overflow (running total) */
+    int64_t list_s;            /* OGX_SOFT_SPLINE: (leaf, leaf) pairs the far field takes within the support */
 } ogx_stats;
 
-/* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0. */
+/* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0,
+ * Plummer softening. */
 int ogx_params_default(ogx_params* prm);
 
 /* Constructor: AdaptiveFMM3D(KernelParams3D, int p, int threshold) (src3d/AdaptiveFMM3D.hpp:22-23)

@@ -226,6 +226,11 @@ static int eval_device_on(Handle& h, int64_t n, const double* d_pos, const doubl
     // beside the U/W/X list build
     if (h.prm.precision == OGX_PREC_MIXED) OGX_TRY(fmm_mixed_m2l(h, d_pot != nullptr));
     OGX_TRY(lists_build_uwx(h));
+    h.soft_pairs = 0;
+    if (h.prm.softening == OGX_SOFT_SPLINE && h.prm.eps > 0.0) {
+        OGX_TRY(soft_lists_build(h));
+        h.stats.list_s = h.soft_pairs;
+    }
     OGX_CUDA(timing_record(h, h.ev[9], st));
     h.tree_valid = true;
     // an eager evaluation has read its counts back by now: capacities for capacity mode
@@ -389,7 +394,10 @@ int step_member(Handle& h, double dt) {
     // a step on the legacy or per-thread default stream cannot be captured: such a handle
     // steps eagerly
     const bool capturable = h.stream != nullptr && h.stream != cudaStreamLegacy && h.stream != cudaStreamPerThread;
-    const bool graphed = h.capture_steps && capturable && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid;
+    // (the spline kernel's S lists are sized by a count read back in the middle of the
+    // evaluation, so such steps stay eager)
+    const bool graphed = h.capture_steps && capturable && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid &&
+                         h.prm.softening == OGX_SOFT_PLUMMER;
     if (!graphed) {
         h.cap_mode = false;
         OGX_TRY(step_once(h, dp, dv, dm, da, dn, dt));
@@ -564,6 +572,7 @@ int ogx_create(const ogx_params* prm, void** handle) {
     if (prm->solver != OGX_SOLVER_ADAPTIVE_FMM && prm->solver != OGX_SOLVER_DIRECT) return OGX_ERR_INVALID;
     if (prm->precision != OGX_PREC_FP64 && prm->precision != OGX_PREC_MIXED && prm->precision != OGX_PREC_FP64_ROT)
         return OGX_ERR_INVALID;
+    if (prm->softening != OGX_SOFT_PLUMMER && prm->softening != OGX_SOFT_SPLINE) return OGX_ERR_INVALID;
     if (prm->solver == OGX_SOLVER_ADAPTIVE_FMM) {
         if (prm->p < 1 || prm->p > kPMax) return OGX_ERR_INVALID;
         if (prm->leaf_capacity < 1 || prm->leaf_capacity > 4096) return OGX_ERR_INVALID;

@@ -8,16 +8,20 @@
 // (|d|^2+eps^2)^{-3/2} is formed from the double-precision rsqrt cubed.
 // The optional potential is pot_i = -G sum_{j != i} m_j / sqrt(|d|^2 + eps^2)
 // (Kernel3D.hpp:39-42 per body, without the m_i factor).
+// With OGX_SOFT_SPLINE every pair takes the spline kernel (ogx_softening.cuh) instead.
 #include "ogx_internal.cuh"
+#include "ogx_softening.cuh"
 
 namespace ogx {
 namespace {
 
 constexpr int DT = 256;
 
-template <class T, bool POT>
+// SOFT: the spline kernel of support hs (ogx_softening.cuh) instead of Plummer's eps2
+template <class T, bool POT, bool SOFT = false>
 __global__ void __launch_bounds__(DT) k_direct(const double* __restrict__ pos, const double* __restrict__ mass, int64_t n, T G,
-                                               T eps2, double* __restrict__ acc, double* __restrict__ pot) {
+                                               T eps2, double* __restrict__ acc, double* __restrict__ pot, T hs = 0,
+                                               T hinv = 0) {
     __shared__ T s[DT][4];
     const int64_t i = blockIdx.x * (int64_t)DT + threadIdx.x;
     const bool act = i < n;
@@ -41,21 +45,37 @@ __global__ void __launch_bounds__(DT) k_direct(const double* __restrict__ pos, c
             for (int k = 0; k < lim; ++k) {
                 if (t0 + k == i) continue;
                 const T dx = s[k][0] - xi, dy = s[k][1] - yi, dz = s[k][2] - zi;
-                const T r2 = dx * dx + dy * dy + dz * dz + eps2;
-                const T ir = rsqrt(r2);
-                const T w = s[k][3] * ir * ir * ir;
-                ax += w * dx; ay += w * dy; az += w * dz;
-                if (POT) ph += s[k][3] * ir;
+                if constexpr (SOFT) {
+                    T g, kk;
+                    spline_gk<T>(dx * dx + dy * dy + dz * dz, hs, hinv, g, kk);
+                    const T w = s[k][3] * g;
+                    ax += w * dx; ay += w * dy; az += w * dz;
+                    if (POT) ph += s[k][3] * kk;
+                } else {
+                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T ir = rsqrt(r2);
+                    const T w = s[k][3] * ir * ir * ir;
+                    ax += w * dx; ay += w * dy; az += w * dz;
+                    if (POT) ph += s[k][3] * ir;
+                }
             }
         } else {
 #pragma unroll 4
             for (int k = 0; k < lim; ++k) {
                 const T dx = s[k][0] - xi, dy = s[k][1] - yi, dz = s[k][2] - zi;
-                const T r2 = dx * dx + dy * dy + dz * dz + eps2;
-                const T ir = rsqrt(r2);
-                const T w = s[k][3] * ir * ir * ir;
-                ax += w * dx; ay += w * dy; az += w * dz;
-                if (POT) ph += s[k][3] * ir;
+                if constexpr (SOFT) {
+                    T g, kk;
+                    spline_gk<T>(dx * dx + dy * dy + dz * dz, hs, hinv, g, kk);
+                    const T w = s[k][3] * g;
+                    ax += w * dx; ay += w * dy; az += w * dz;
+                    if (POT) ph += s[k][3] * kk;
+                } else {
+                    const T r2 = dx * dx + dy * dy + dz * dz + eps2;
+                    const T ir = rsqrt(r2);
+                    const T w = s[k][3] * ir * ir * ir;
+                    ax += w * dx; ay += w * dy; az += w * dz;
+                    if (POT) ph += s[k][3] * ir;
+                }
             }
         }
     }
@@ -84,6 +104,14 @@ int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n,
     if (n == 0) return OGX_OK;
     const int grid = (int)((n + DT - 1) / DT);
     const double eps2 = h.prm.eps * h.prm.eps;
+    if (h.prm.softening == OGX_SOFT_SPLINE && !fp32) {
+        const double hs = spline_support(h.prm.eps), hinv = hs > 0.0 ? 1.0 / hs : 0.0;
+        if (d_pot) k_direct<double, true, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, d_pot, hs, hinv);
+        else k_direct<double, false, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, h.prm.G, eps2, d_acc, nullptr, hs, hinv);
+        ++h.launches;
+        OGX_CUDA(cudaGetLastError());
+        return OGX_OK;
+    }
     if (fp32) {
         if (d_pot) { k_direct<float, true><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, d_pot); ++h.launches; }
         else { k_direct<float, false><<<grid, DT, 0, h.stream>>>(d_pos, d_mass, n, (float)h.prm.G, (float)eps2, d_acc, nullptr); ++h.launches; }

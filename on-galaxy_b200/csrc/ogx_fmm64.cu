@@ -416,8 +416,9 @@ __global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uin
 }
 
 // ---- leaf near field (P2P over U) + final combine ----------------------------------------
-template <bool POT>
-__global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot) {
+template <bool POT, bool SOFT = false>
+__global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot,
+                                                   double hs = 0.0, double hinv = 0.0) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int lf = blockIdx.x * 4 + wid;
     if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
@@ -434,13 +435,24 @@ __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double
             const int s0 = tv.pfirst[c], sc = tv.pcount[c];
             for (int j = s0; j < s0 + sc; ++j) {
                 const double dx = __ldg(tv.px + j) - x, dy = __ldg(tv.py + j) - y, dz = __ldg(tv.pz + j) - z;
-                const double r2 = (dx * dx + dy * dy + dz * dz) + eps2;
-                const double ir = rsqrt(r2);
                 const double mj = (j == i) ? 0.0 : __ldg(tv.pm + j);
-                const double w = mj * ir * ir * ir;
-                if (j != i) {
-                    ax = fma(w, dx, ax); ay = fma(w, dy, ay); az = fma(w, dz, az);
-                    if (POT) ph = fma(mj, ir, ph);
+                if constexpr (SOFT) {
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    double g, k;
+                    spline_gk<double>(j == i ? 1.0 : r2, hs, hinv, g, k);
+                    const double w = mj * g;
+                    if (j != i) {
+                        ax = fma(w, dx, ax); ay = fma(w, dy, ay); az = fma(w, dz, az);
+                        if (POT) ph = fma(mj, k, ph);
+                    }
+                } else {
+                    const double r2 = (dx * dx + dy * dy + dz * dz) + eps2;
+                    const double ir = rsqrt(r2);
+                    const double w = mj * ir * ir * ir;
+                    if (j != i) {
+                        ax = fma(w, dx, ax); ay = fma(w, dy, ay); az = fma(w, dz, az);
+                        if (POT) ph = fma(mj, ir, ph);
+                    }
                 }
             }
         }
@@ -453,6 +465,69 @@ __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double
         }
     }
 }
+
+// ---- OGX_SOFT_SPLINE: the far field's pairs within the support ------------------------
+// For each leaf b and each leaf c of its S list (not adjacent to b, within the support hs),
+// out[4 i] += sum_j m_j (g(r) - r^-3) (r_j - r_i) and, for potentials, m_j (k(r) - 1/r),
+// over the pairs closer than hs (the difference is zero beyond).  The far field took these
+// pairs with the Newtonian kernel; with this sum they carry the spline kernel's force.
+// Warp per leaf, lanes over the leaf's bodies, FP64, in both forms.
+template <bool POT>
+__global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, double hs, double hinv, double* out) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lf = blockIdx.x * 4 + wid;
+    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
+    const int64_t e0 = tv.s_off[lf], e1 = tv.s_off[lf + 1];
+    if (e0 == e1) return;
+    const int b = tv.leafbox[lf];
+    const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
+    const double hs2 = hs * hs;
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int jj = j0 + lane;
+        const bool act = jj < cnt;
+        const int i = f0 + (act ? jj : 0);
+        const double x = tv.px[i], y = tv.py[i], z = tv.pz[i];
+        double ax = 0, ay = 0, az = 0, ph = 0;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int c = tv.s_idx[e];
+            const int s0 = tv.pfirst[c], sc = tv.pcount[c];
+            for (int j = s0; j < s0 + sc; ++j) {
+                const double dx = __ldg(tv.px + j) - x, dy = __ldg(tv.py + j) - y, dz = __ldg(tv.pz + j) - z;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 < hs2 && r2 > 0.0) {
+                    double g, k;
+                    spline_gk<double>(r2, hs, hinv, g, k);
+                    const double ir = rsqrt(r2);
+                    const double mj = __ldg(tv.pm + j);
+                    const double w = mj * (g - ir * ir * ir);
+                    ax = fma(w, dx, ax); ay = fma(w, dy, ay); az = fma(w, dz, az);
+                    if (POT) ph = fma(mj, k - ir, ph);
+                }
+            }
+        }
+        if (act) {
+            out[4 * (size_t)i] += ax;
+            out[4 * (size_t)i + 1] += ay;
+            out[4 * (size_t)i + 2] += az;
+            if (POT) out[4 * (size_t)i + 3] += ph;
+        }
+    }
+}
+
+}  // namespace
+
+int soft_correct_launch(Handle& h, double* out, bool pot, cudaStream_t st) {
+    const TreeView& tv = h.tv;
+    if (h.soft_pairs == 0 || tv.nleaf == 0) return OGX_OK;
+    const double hs = spline_support(h.prm.eps), hinv = 1.0 / hs;
+    if (pot) k_soft_correct<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hs, hinv, out);
+    else k_soft_correct<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hs, hinv, out);
+    ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
+
+namespace {
 
 // ---- dispatch --------------------------------------------------------------------------
 template <int P>
@@ -497,7 +572,14 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     const bool pot = d_pot != nullptr;
     OGX_TRY((launch_far<P, double>(h, M, L, far, pot)));
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
-    if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
+    if (h.prm.softening == OGX_SOFT_SPLINE) {
+        // the far field's pairs within the support, then the spline kernel in the near field
+        OGX_TRY(soft_correct_launch(h, far, pot, st));
+        const double hs = spline_support(h.prm.eps), hinv = hs > 0.0 ? 1.0 / hs : 0.0;
+        if (pot) k_leaf_near<true, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot, hs, hinv);
+        else k_leaf_near<false, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr, hs, hinv);
+        ++h.launches;
+    } else if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
     else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
     OGX_CUDA(timing_record(h, h.ev[7], st));
     OGX_CUDA(cudaGetLastError());
@@ -705,9 +787,20 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         OGX_TRY(launch_far32_m2p<P>(h, M, far_m, d_pot != nullptr, h.side));
         mixed::k_near_prep<<<(tv.n + 255) / 256, 256, 0, h.side>>>(tv, rel, rel + tv.n); ++h.launches;
         const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
-        auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32> : mixed::k_leaf_near32<true, 64>)
-                          : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32> : mixed::k_leaf_near32<false, 64>);
-        near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb); ++h.launches;
+        if (h.prm.softening == OGX_SOFT_SPLINE) {
+            // spline kernel in the near field; the far field's pairs within the support are
+            // corrected into the M2P part (written above on this stream)
+            const double hs = spline_support(h.prm.eps);
+            const float hsf = (float)hs, hinvf = hs > 0.0 ? (float)(1.0 / hs) : 0.f;
+            auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32, true> : mixed::k_leaf_near32<true, 64, true>)
+                              : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32, true> : mixed::k_leaf_near32<false, 64, true>);
+            near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb, hsf, hinvf); ++h.launches;
+            OGX_TRY(soft_correct_launch(h, far_m, d_pot != nullptr, h.side));
+        } else {
+            auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32> : mixed::k_leaf_near32<true, 64>)
+                              : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32> : mixed::k_leaf_near32<false, 64>);
+            near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb, 0.f, 0.f); ++h.launches;
+        }
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }
     // join the M2L (its end is timing event 4, recorded on h.m2l)

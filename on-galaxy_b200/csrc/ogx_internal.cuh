@@ -79,7 +79,7 @@ enum Slot {
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_MUNSCALE, S_MIX_OUNSCALE, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,
     S_NEAR32, S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
-    S_ROT_PACK, S_TR_READY_M, S_TR_READY_L,
+    S_ROT_PACK, S_TR_READY_M, S_TR_READY_L, S_SOFT_CNT, S_SOFT_OFF, S_SOFT_IDX,
     S_NUM_SLOTS
 };
 
@@ -187,6 +187,10 @@ struct TreeView {
     const int *u_idx, *w_idx;
     const int64_t* x_off;              // per box (nb+1)
     const int* x_idx;
+    // OGX_SOFT_SPLINE: per leaf, the leaves that are not adjacent to it (so the far field
+    // takes their pairs) but lie within the spline's support of it (nleaf+1 offsets)
+    const int64_t* s_off;
+    const int* s_idx;
 };
 
 #ifdef __CUDACC__
@@ -243,6 +247,7 @@ struct Handle {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_in = nullptr, ev_out = nullptr, ev_tree = nullptr, ev_up = nullptr;
     cudaEvent_t ev_up_end = nullptr;   // timing: end of an upward pass that ran on `up`
     bool upward_split = false;         // the last evaluation ran its upward pass on `up`
+    int64_t soft_pairs = 0;            // OGX_SOFT_SPLINE: S-list entries of the last evaluation
     TreeView tv{};
     bool tree_valid = false;
     // mixed-precision tables
@@ -307,6 +312,8 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n);
 int lists_build(Handle& h);           // both parts below, in order
 int lists_build_targets(Handle& h);   // colleagues; M2L target tiles on `aux`
 int lists_build_uwx(Handle& h);       // U, W and X lists
+int soft_lists_build(Handle& h);      // OGX_SOFT_SPLINE: the leaf pairs the far field takes within the support
+int soft_correct_launch(Handle& h, double* out, bool pot, cudaStream_t st);   // adds the kernel difference over them
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int m2l_rot_launch(Handle& h, const double* M, double* Lown);   // third form's M2L, on h.stream

@@ -22,6 +22,7 @@
 #include <algorithm>
 
 #include "ogx_tree_common.cuh"
+#include "ogx_softening.cuh"
 
 namespace ogx {
 namespace {
@@ -350,7 +351,86 @@ inline int bits_for(int64_t v) {
     return b;
 }
 
+// OGX_SOFT_SPLINE: for each leaf b, the leaves c that are not adjacent to b (the far
+// field takes their pairs) and whose box lies within the spline's support `hs` of b's
+// box, found by a depth-first walk from the root that skips every box farther than hs.
+// Adjacency is the U-list predicate (AdaptiveOctree::adjacent, same FP64 operations), so
+// every leaf pair is either in b's U list or a candidate here.  Thread per leaf; pass 1
+// counts, pass 2 writes in the same order.
+constexpr int kSoftStack = 8 * (kMaxDepth + 2);   // > 7 per level + 8: the walk never overflows it
+template <bool EMIT>
+__global__ void __launch_bounds__(128) k_soft_lists(int nleaf, const int* __restrict__ leafbox, const int* __restrict__ child,
+                                                    const int* __restrict__ leafid, const double* __restrict__ ctr,
+                                                    const RootInfo* __restrict__ root, double hs, int* cnt,
+                                                    const int64_t* __restrict__ off, int* idx, const DevCounts* counts) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= nleaf) return;
+    if (lf >= counts->nleaf32 || counts->overflow) {
+        if (!EMIT) cnt[lf] = 0;
+        return;
+    }
+    const int b = leafbox[lf];
+    const double tol = root->tol;
+    const double bx = ctr[4 * b], by = ctr[4 * b + 1], bz = ctr[4 * b + 2], bh = ctr[4 * b + 3];
+    const double hs2 = hs * hs;
+    int stack[kSoftStack];
+    int sp = 0, n = 0;
+    const int64_t o = EMIT ? off[lf] : 0;
+    stack[sp++] = 0;   // the root
+    while (sp > 0) {
+        const int c = stack[--sp];
+        const double ch = ctr[4 * c + 3];
+        // gap between the two boxes along each axis (0 where they overlap)
+        const double gx = fmax(0.0, fabs(ctr[4 * c] - bx) - (ch + bh));
+        const double gy = fmax(0.0, fabs(ctr[4 * c + 1] - by) - (ch + bh));
+        const double gz = fmax(0.0, fabs(ctr[4 * c + 2] - bz) - (ch + bh));
+        if (gx * gx + gy * gy + gz * gz >= hs2) continue;
+        if (leafid[c] >= 0) {
+            const double lim = __dadd_rn(__dadd_rn(ch, bh), tol);
+            const bool adj = fabs(__dsub_rn(ctr[4 * c], bx)) <= lim && fabs(__dsub_rn(ctr[4 * c + 1], by)) <= lim &&
+                             fabs(__dsub_rn(ctr[4 * c + 2], bz)) <= lim;
+            if (!adj) {
+                if (EMIT) idx[o + n] = c;
+                ++n;
+            }
+        } else {
+            for (int s = 7; s >= 0; --s) {
+                const int k = child[8 * c + s];
+                if (k >= 0 && sp < kSoftStack) stack[sp++] = k;
+            }
+        }
+    }
+    if (!EMIT) cnt[lf] = n;
+}
+
 }  // namespace
+
+// Built after the U/W/X lists of an eager evaluation (one more count read-back).
+int soft_lists_build(Handle& h) {
+    const cudaStream_t st = h.stream;
+    TreeView& tv = h.tv;
+    const int nleaf = tv.nleaf;
+    int* cnt;
+    int64_t* off;
+    OGX_TRY(arena_get(h.ws, S_SOFT_CNT, nleaf, &cnt));
+    OGX_TRY(arena_get(h.ws, S_SOFT_OFF, nleaf + 1, &off));
+    const double hs = spline_support(h.prm.eps);
+    k_soft_lists<false><<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, tv.child, tv.leafid, tv.center, tv.root, hs,
+                                                              cnt, nullptr, nullptr, h.d_counts); ++h.launches;
+    OGX_TRY(scan_i32_to_i64(h, cnt, off, nleaf));
+    int64_t ns = 0;
+    OGX_CUDA(cudaMemcpyAsync(&ns, off + nleaf, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    OGX_CUDA(cudaStreamSynchronize(st));
+    int* idx;
+    OGX_TRY(arena_get(h.ws, S_SOFT_IDX, ns + 1, &idx));
+    k_soft_lists<true><<<grid_for(nleaf, 128), 128, 0, st>>>(nleaf, tv.leafbox, tv.child, tv.leafid, tv.center, tv.root, hs,
+                                                             nullptr, off, idx, h.d_counts); ++h.launches;
+    tv.s_off = off;
+    tv.s_idx = idx;
+    h.soft_pairs = ns;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
 
 int lists_build(Handle& h) {
     OGX_TRY(lists_build_targets(h));

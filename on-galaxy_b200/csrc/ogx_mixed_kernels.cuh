@@ -56,6 +56,7 @@
 
 #include "ogx_harmonics.cuh"
 #include "ogx_sm100.cuh"
+#include "ogx_softening.cuh"
 
 namespace ogx {
 namespace mixed {
@@ -649,10 +650,12 @@ __global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restri
 }
 
 // softened pair sum of one target over staged sources q = q0, q0 + dq, ... < n;
-// SELF: the source at staged position self_q is the target itself and is skipped
-template <bool SELF, bool POT>
+// SELF: the source at staged position self_q is the target itself and is skipped.
+// SOFT: the spline kernel of support hs (ogx_softening.cuh) instead of Plummer's eps2
+template <bool SELF, bool POT, bool SOFT = false>
 __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const float4* __restrict__ slo, int q0, int dq, int n,
-                                         int self_q, const float (&th)[3], const float (&tl)[3], float eps2, float (&a)[4]) {
+                                         int self_q, const float (&th)[3], const float (&tl)[3], float eps2, float (&a)[4],
+                                         float hs = 0.f, float hinv = 0.f) {
 #pragma unroll 4
     for (int q = q0; q < n; q += dq) {
         const float4 h = shi[q];
@@ -660,17 +663,29 @@ __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const f
         const float dx = (h.x - th[0]) + (l.x - tl[0]);
         const float dy = (h.y - th[1]) + (l.y - tl[1]);
         const float dz = (h.z - th[2]) + (l.z - tl[2]);
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
         const bool self = SELF && (q == self_q);
-        // rsqrtf alone (within 2 ulp): its error, ~1e-7 per pair in random directions,
-        // stays far below the form's budget
-        const float y = rsqrtf(self ? 1.0f : r2);
-        const float my = (self ? 0.0f : h.w) * y;
-        const float w = my * y * y;
-        a[0] = fmaf(w, dx, a[0]);
-        a[1] = fmaf(w, dy, a[1]);
-        a[2] = fmaf(w, dz, a[2]);
-        if (POT) a[3] += my;
+        if constexpr (SOFT) {
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float g, k;
+            spline_gk<float>(self ? 1.0f : r2, hs, hinv, g, k);
+            const float m = self ? 0.0f : h.w;
+            const float w = m * g;
+            a[0] = fmaf(w, dx, a[0]);
+            a[1] = fmaf(w, dy, a[1]);
+            a[2] = fmaf(w, dz, a[2]);
+            if (POT) a[3] = fmaf(m, k, a[3]);
+        } else {
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+            // rsqrtf alone (within 2 ulp): its error, ~1e-7 per pair in random directions,
+            // stays far below the form's budget
+            const float y = rsqrtf(self ? 1.0f : r2);
+            const float my = (self ? 0.0f : h.w) * y;
+            const float w = my * y * y;
+            a[0] = fmaf(w, dx, a[0]);
+            a[1] = fmaf(w, dy, a[1]);
+            a[2] = fmaf(w, dz, a[2]);
+            if (POT) a[3] += my;
+        }
     }
 }
 
@@ -700,9 +715,10 @@ __device__ __forceinline__ int near_parts(int T) {
 // are added in part order in FP64 through shared memory (deterministic).  Output:
 // near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64.  The kernel needs
 // only the tree and the lists, so it runs beside the far-field chain.
-template <bool POT, int NU>
+template <bool POT, int NU, bool SOFT = false>
 __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float4* __restrict__ rhi,
-                                                        const float4* __restrict__ rlo, float eps2, double* __restrict__ near) {
+                                                        const float4* __restrict__ rlo, float eps2, double* __restrict__ near,
+                                                        float hs = 0.f, float hinv = 0.f) {
     constexpr int R = NU / 32;
     static_assert(R * 32 == NU && R >= 1 && R <= 2, "near-field units: 32 or 64");
     __shared__ float4 s_hi[NEAR_CAP], s_lo[NEAR_CAP];
@@ -750,7 +766,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                 for (int r = 0; r < R; ++r) {
                     if (!act[r]) continue;
                     float a[4] = {0.f, 0.f, 0.f, 0.f};
-                    p2p_part<true, POT>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a);
+                    p2p_part<true, POT, SOFT>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a, hs, hinv);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
                         if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);
@@ -797,7 +813,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                     for (int r = 0; r < R; ++r) {
                         if (!act[r]) continue;
                         float a[4] = {0.f, 0.f, 0.f, 0.f};
-                        p2p_part<false, POT>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a);
+                        p2p_part<false, POT, SOFT>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a, hs, hinv);
 #pragma unroll
                         for (int k = 0; k < 4; ++k)
                             if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);

@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "libogx.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_NO_DEVICE, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_STATE = range(8)
 SOLVER_ADAPTIVE_FMM, SOLVER_DIRECT = 0, 1
 PREC_FP64, PREC_MIXED, PREC_FP64_ROT = 0, 1, 2
+SOFT_PLUMMER, SOFT_SPLINE = 0, 1
 
 # Every entry point declared in include/ogx.h (checked by the ABI test).
 EXPORTS = (
@@ -39,7 +40,8 @@ EXPORTS = (
 
 class Params(C.Structure):
     _fields_ = [("G", C.c_double), ("eps", C.c_double), ("p", C.c_int), ("leaf_capacity", C.c_int),
-                ("solver", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("stream", C.c_void_p)]
+                ("solver", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("stream", C.c_void_p),
+                ("softening", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -51,7 +53,7 @@ class Stats(C.Structure):
                 ("ms_tree", C.c_double), ("ms_lists", C.c_double), ("ms_upward", C.c_double), ("ms_m2l", C.c_double),
                 ("ms_p2l", C.c_double), ("ms_downward", C.c_double), ("ms_leaf", C.c_double), ("ms_total", C.c_double),
                 ("ms_h2d", C.c_double), ("ms_d2h", C.c_double), ("launches", C.c_int64),
-                ("graph_steps", C.c_int64), ("step_redos", C.c_int64)]
+                ("graph_steps", C.c_int64), ("step_redos", C.c_int64), ("list_s", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -161,13 +163,14 @@ def direct_eval_noalloc(pos, mass, G=1.0, eps=0.0, with_pot=False, stream=None):
 
 class _Solver:
     def __init__(self, G=1.0, eps=0.0, p=8, threshold=64, solver=SOLVER_ADAPTIVE_FMM, precision=PREC_FP64,
-                 device=0, stream=None):
+                 device=0, stream=None, softening=SOFT_PLUMMER):
         lib = load()
         prm = Params()
         lib.ogx_params_default(C.byref(prm))
         prm.G, prm.eps, prm.p, prm.leaf_capacity = float(G), float(eps), int(p), int(threshold)
         prm.solver, prm.precision, prm.device = int(solver), int(precision), int(device)
         prm.stream = stream
+        prm.softening = int(softening)
         h = C.c_void_p()
         _check(lib.ogx_create(C.byref(prm), C.byref(h)), "ogx_create")
         self._h = h
@@ -315,12 +318,13 @@ class _Solver:
 class AdaptiveFMM3D(_Solver):
     """Drop-in for galaxy3d::AdaptiveFMM3D(KernelParams3D{G, eps}, p, threshold)."""
 
-    def __init__(self, G=1.0, eps=0.0, p=8, threshold=64, precision=PREC_FP64, device=0, stream=None):
-        super().__init__(G, eps, p, threshold, SOLVER_ADAPTIVE_FMM, precision, device, stream)
+    def __init__(self, G=1.0, eps=0.0, p=8, threshold=64, precision=PREC_FP64, device=0, stream=None,
+                 softening=SOFT_PLUMMER):
+        super().__init__(G, eps, p, threshold, SOLVER_ADAPTIVE_FMM, precision, device, stream, softening)
 
 
 class DirectSolver3D(_Solver):
     """Drop-in for galaxy3d::DirectSolver3D(KernelParams3D{G, eps})."""
 
-    def __init__(self, G=1.0, eps=0.0, device=0, stream=None):
-        super().__init__(G, eps, 8, 64, SOLVER_DIRECT, PREC_FP64, device, stream)
+    def __init__(self, G=1.0, eps=0.0, device=0, stream=None, softening=SOFT_PLUMMER):
+        super().__init__(G, eps, 8, 64, SOLVER_DIRECT, PREC_FP64, device, stream, softening)
