@@ -49,7 +49,8 @@ public:
         return acc;
     }
 
-    // Accelerations and per-body potentials pot_i = -G sum_j m_j / sqrt(r_ij^2 + eps^2).
+    // Accelerations and per-body potentials pot_i = -G sum_j m_j / sqrt(r_ij^2 + eps^2)
+    // (the spline kernel's potential with OGX_SOFT_SPLINE).
     galaxy3d::Accelerations3D computePotentials(const galaxy3d::Bodies3D& bodies, std::vector<double>& pot) const {
         galaxy3d::Accelerations3D acc(bodies.size());
         pot.assign(bodies.size(), 0.0);
@@ -65,7 +66,8 @@ public:
     const ogx_stats& lastStats() const { return stats_; }
 
 protected:
-    OgxSolver3D(const galaxy3d::KernelParams3D& k, int solver, int p, int threshold, int precision, int device) {
+    OgxSolver3D(const galaxy3d::KernelParams3D& k, int solver, int p, int threshold, int precision, int device,
+                int softening = OGX_SOFT_PLUMMER) {
         ogx_params prm;
         ogx_params_default(&prm);
         prm.G = k.G;
@@ -75,6 +77,7 @@ protected:
         prm.solver = solver;
         prm.precision = precision;
         prm.device = device;
+        prm.softening = softening;
         check(ogx_create(&prm, &h_), "ogx_create");
     }
 
@@ -102,16 +105,18 @@ private:
 // AdaptiveFMM3D(KernelParams3D kp, int p, int threshold = 64)
 class OgxAdaptiveFMM3D : public OgxSolver3D {
 public:
+    // softening = OGX_SOFT_SPLINE: compact spline kernel with the far field corrected
+    // within its support (an extension; the default is the reference's Plummer kernel)
     OgxAdaptiveFMM3D(const galaxy3d::KernelParams3D& k, int p, int threshold = 64, int precision = OGX_PREC_FP64,
-                     int device = 0)
-        : OgxSolver3D(k, OGX_SOLVER_ADAPTIVE_FMM, p, threshold, precision, device) {}
+                     int device = 0, int softening = OGX_SOFT_PLUMMER)
+        : OgxSolver3D(k, OGX_SOLVER_ADAPTIVE_FMM, p, threshold, precision, device, softening) {}
 };
 
 // DirectSolver3D(KernelParams3D kp)
 class OgxDirect3D : public OgxSolver3D {
 public:
-    explicit OgxDirect3D(const galaxy3d::KernelParams3D& k, int device = 0)
-        : OgxSolver3D(k, OGX_SOLVER_DIRECT, 8, 64, OGX_PREC_FP64, device) {}
+    explicit OgxDirect3D(const galaxy3d::KernelParams3D& k, int device = 0, int softening = OGX_SOFT_PLUMMER)
+        : OgxSolver3D(k, OGX_SOLVER_DIRECT, 8, 64, OGX_PREC_FP64, device, softening) {}
 };
 
 }  // namespace ogx_b200

@@ -12,7 +12,10 @@
 // instead of the reference's O(N^2) pair sum, so they are available at any N.
 //
 // usage: ogx_galaxy_sim [--N n_per_galaxy] [--steps S] [--dt DT] [--stride F] [--p P]
-//                       [--thr T] [--eps E] [--seed S] [--precision fp64|fp64rot|mixed] [--out PREFIX]
+//                       [--thr T] [--eps E] [--seed S] [--precision fp64|fp64rot|mixed]
+//                       [--softening plummer|spline] [--out PREFIX]
+// --softening spline: compact spline kernel with the far field corrected within its
+// support (OGX_SOFT_SPLINE), instead of the reference's Plummer kernel in P2P only.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -40,6 +43,7 @@ int main(int argc, char** argv) {
     double dt = 0.01, eps = 0.05;
     uint64_t seed = 1;
     int precision = OGX_PREC_MIXED;
+    int softening = OGX_SOFT_PLUMMER;
     std::string out = "merger";
     for (int i = 1; i + 1 < argc; i += 2) {
         const std::string a = argv[i], v = argv[i + 1];
@@ -60,6 +64,14 @@ int main(int argc, char** argv) {
                 return 2;
             }
         }
+        else if (a == "--softening") {
+            if (v == "plummer") softening = OGX_SOFT_PLUMMER;
+            else if (v == "spline") softening = OGX_SOFT_SPLINE;
+            else {
+                std::fprintf(stderr, "unknown softening '%s' (expected plummer or spline)\n", v.c_str());
+                return 2;
+            }
+        }
         else if (a == "--out") out = v;
         else {
             std::fprintf(stderr, "unknown option %s\n", a.c_str());
@@ -76,6 +88,7 @@ int main(int argc, char** argv) {
     prm.p = p;
     prm.leaf_capacity = thr;
     prm.precision = precision;
+    prm.softening = softening;
     void* h = nullptr;
     int rc = ogx_create(&prm, &h);
     if (rc != OGX_OK) return fail(rc, "ogx_create");

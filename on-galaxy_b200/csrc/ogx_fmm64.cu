@@ -471,7 +471,8 @@ __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double
 // out[4 i] += sum_j m_j (g(r) - r^-3) (r_j - r_i) and, for potentials, m_j (k(r) - 1/r),
 // over the pairs closer than hs (the difference is zero beyond).  The far field took these
 // pairs with the Newtonian kernel; with this sum they carry the spline kernel's force.
-// Warp per leaf, lanes over the leaf's bodies, FP64, in both forms.
+// Warp per leaf, lanes over the leaf's bodies, FP64 (the plain form; the mixed form runs
+// the FP32 near-field kernel over the same lists, mixed::k_leaf_near32<.., 2>).
 template <bool POT>
 __global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, double hs, double hinv, double* out) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -770,6 +771,13 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_FAR_M, 4 * (size_t)tv.n, &far_m));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
+    // near-field work items (leaf, chunk of 32 targets): counts and offsets
+    int* nchunk;
+    int64_t* chunk_off;
+    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK, (size_t)tv.nleaf, &nchunk));
+    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK_OFF, (size_t)tv.nleaf + 1, &chunk_off));
+    mixed::k_near_chunks<<<(tv.nleaf + 255) / 256, 256, 0, st>>>(tv, nchunk); ++h.launches;
+    OGX_TRY(scan_i32_to_i64(h, nchunk, chunk_off, tv.nleaf));
     // join the upward pass (the side stream's M2P reads the multipoles)
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
     // the far field's M2P part and the near field need the tree, the multipoles and the
@@ -786,20 +794,27 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
         // the far field's M2P part (multipoles only) first, then the near field
         OGX_TRY(launch_far32_m2p<P>(h, M, far_m, d_pot != nullptr, h.side));
         mixed::k_near_prep<<<(tv.n + 255) / 256, 256, 0, h.side>>>(tv, rel, rel + tv.n); ++h.launches;
-        const int ngrid = tv.nleaf;   // one block per leaf (a bounded grid left the far chain waiting)
+        // one block per work item: the leaves' chunks number at most nleaf + n / 32 (a
+        // bounded grid left the far chain waiting)
+        const int ngrid = tv.nleaf + (tv.n + 31) / 32;
         if (h.prm.softening == OGX_SOFT_SPLINE) {
             // spline kernel in the near field; the far field's pairs within the support are
-            // corrected into the M2P part (written above on this stream)
+            // corrected in FP32 into the M2P part (written above on this stream)
             const double hs = spline_support(h.prm.eps);
             const float hsf = (float)hs, hinvf = hs > 0.0 ? (float)(1.0 / hs) : 0.f;
-            auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32, true> : mixed::k_leaf_near32<true, 64, true>)
-                              : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32, true> : mixed::k_leaf_near32<false, 64, true>);
-            near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb, hsf, hinvf); ++h.launches;
-            OGX_TRY(soft_correct_launch(h, far_m, d_pot != nullptr, h.side));
+            auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32, 1> : mixed::k_leaf_near32<true, 64, 1>)
+                              : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32, 1> : mixed::k_leaf_near32<false, 64, 1>);
+            near<<<ngrid, 32, 0, h.side>>>(tv, chunk_off, rel, rel + tv.n, eps2, nearb, hsf, hinvf); ++h.launches;
+            if (h.soft_pairs > 0) {
+                // the same staging over the S lists, the kernel difference added into far_m
+                auto corr = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32, 2> : mixed::k_leaf_near32<true, 64, 2>)
+                                  : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32, 2> : mixed::k_leaf_near32<false, 64, 2>);
+                corr<<<ngrid, 32, 0, h.side>>>(tv, chunk_off, rel, rel + tv.n, eps2, far_m, hsf, hinvf); ++h.launches;
+            }
         } else {
             auto near = d_pot ? (h.near_units == 32 ? mixed::k_leaf_near32<true, 32> : mixed::k_leaf_near32<true, 64>)
                               : (h.near_units == 32 ? mixed::k_leaf_near32<false, 32> : mixed::k_leaf_near32<false, 64>);
-            near<<<ngrid, 32, 0, h.side>>>(tv, rel, rel + tv.n, eps2, nearb, 0.f, 0.f); ++h.launches;
+            near<<<ngrid, 32, 0, h.side>>>(tv, chunk_off, rel, rel + tv.n, eps2, nearb, 0.f, 0.f); ++h.launches;
         }
         OGX_CUDA(cudaEventRecord(h.ev_join, h.side));
     }

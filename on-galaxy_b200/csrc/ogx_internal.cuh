@@ -79,7 +79,7 @@ enum Slot {
     S_MIX_POS4, S_MIX_MHI, S_MIX_MLO, S_MIX_MUNSCALE, S_MIX_OUNSCALE, S_MIX_TOPS, S_MIX_LOWN, S_MIX_ROW0, S_ERR, S_EVAL_H, S_EVAL_G, S_UW_LANE,
     S_NONLEAF_FLAG, S_NONLEAF_OFF, S_NONLEAF, S_NONLEAF_LOFF, S_FAR_HEAVY,
     S_NEAR32, S_SPECIES, S_DIAG_POT, S_DIAG_ACC, S_DIAG_PART, S_FRAME, S_IC_POS, S_IC_MASS, S_IC_ACC,
-    S_ROT_PACK, S_TR_READY_M, S_TR_READY_L, S_SOFT_CNT, S_SOFT_OFF, S_SOFT_IDX,
+    S_ROT_PACK, S_TR_READY_M, S_TR_READY_L, S_SOFT_CNT, S_SOFT_OFF, S_SOFT_IDX, S_NEAR_CHUNK, S_NEAR_CHUNK_OFF,
     S_NUM_SLOTS
 };
 

@@ -640,6 +640,13 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 
 constexpr int NEAR_CAP = 128;    // source bodies staged per round (several U-list entries)
 
+// work items of the near field: ceil(bodies / 32) per leaf (none for capacity padding)
+__global__ void k_near_chunks(TreeView tv, int* __restrict__ cnt) {
+    const int lf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lf >= tv.nleaf) return;
+    cnt[lf] = (lf < tv_nleaf(tv) && !tv_over(tv)) ? (tv.pcount[tv.leafbox[lf]] + 31) / 32 : 0;
+}
+
 __global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restrict__ rhi, float4* __restrict__ rlo) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= tv.n || tv_over(tv)) return;
@@ -651,8 +658,10 @@ __global__ void __launch_bounds__(256) k_near_prep(TreeView tv, float4* __restri
 
 // softened pair sum of one target over staged sources q = q0, q0 + dq, ... < n;
 // SELF: the source at staged position self_q is the target itself and is skipped.
-// SOFT: the spline kernel of support hs (ogx_softening.cuh) instead of Plummer's eps2
-template <bool SELF, bool POT, bool SOFT = false>
+// KM (kernel): 0 Plummer's (eps2); 1 the spline of support hs (ogx_softening.cuh);
+// 2 the spline minus the Newtonian kernel, zero from hs on (the far field's pairs
+// inside the support, OGX_SOFT_SPLINE)
+template <bool SELF, bool POT, int KM = 0>
 __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const float4* __restrict__ slo, int q0, int dq, int n,
                                          int self_q, const float (&th)[3], const float (&tl)[3], float eps2, float (&a)[4],
                                          float hs = 0.f, float hinv = 0.f) {
@@ -664,7 +673,7 @@ __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const f
         const float dy = (h.y - th[1]) + (l.y - tl[1]);
         const float dz = (h.z - th[2]) + (l.z - tl[2]);
         const bool self = SELF && (q == self_q);
-        if constexpr (SOFT) {
+        if constexpr (KM == 1) {
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             float g, k;
             spline_gk<float>(self ? 1.0f : r2, hs, hinv, g, k);
@@ -674,6 +683,18 @@ __device__ __forceinline__ void p2p_part(const float4* __restrict__ shi, const f
             a[1] = fmaf(w, dy, a[1]);
             a[2] = fmaf(w, dz, a[2]);
             if (POT) a[3] = fmaf(m, k, a[3]);
+        } else if constexpr (KM == 2) {
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 < hs * hs && r2 > 0.0f) {
+                float g, k;
+                spline_gk<float>(r2, hs, hinv, g, k);
+                const float y = rsqrtf(r2);
+                const float w = h.w * (g - y * y * y);
+                a[0] = fmaf(w, dx, a[0]);
+                a[1] = fmaf(w, dy, a[1]);
+                a[2] = fmaf(w, dz, a[2]);
+                if (POT) a[3] = fmaf(h.w, k - y, a[3]);
+            }
         } else {
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
             // rsqrtf alone (within 2 ulp): its error, ~1e-7 per pair in random directions,
@@ -715,22 +736,39 @@ __device__ __forceinline__ int near_parts(int T) {
 // are added in part order in FP64 through shared memory (deterministic).  Output:
 // near[4 i] = (sum m d / r^3 xyz, sum m / r) of sorted body i, FP64.  The kernel needs
 // only the tree and the lists, so it runs beside the far-field chain.
-template <bool POT, int NU, bool SOFT = false>
-__global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float4* __restrict__ rhi,
-                                                        const float4* __restrict__ rlo, float eps2, double* __restrict__ near,
-                                                        float hs = 0.f, float hinv = 0.f) {
+// KM = 1: the spline kernel (OGX_SOFT_SPLINE).  KM = 2: the far field's pairs inside the
+// spline's support instead: the leaf's S list in place of its U list (no self round),
+// the kernel difference, and the result added to near[] rather than stored.
+// Work items are (leaf, chunk of 32 targets): chunk_off[lf] is the first item of leaf lf
+// (k_near_chunks + an exclusive scan), so a leaf of many bodies (the eps floor stops
+// splitting in dense cores) spreads over as many blocks as it has chunks.
+template <bool POT, int NU, int KM = 0>
+__global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const int64_t* __restrict__ chunk_off,
+                                                        const float4* __restrict__ rhi, const float4* __restrict__ rlo,
+                                                        float eps2, double* __restrict__ near, float hs = 0.f,
+                                                        float hinv = 0.f) {
     constexpr int R = NU / 32;
     static_assert(R * 32 == NU && R >= 1 && R <= 2, "near-field units: 32 or 64");
     __shared__ float4 s_hi[NEAR_CAP], s_lo[NEAR_CAP];
     __shared__ double s_red[NU][4];
     const int lane = threadIdx.x & 31;
     if (tv_over(tv)) return;
-    const int nleaf = min(tv.nleaf, tv_nleaf(tv));
-    for (int lf = blockIdx.x; lf < nleaf; lf += gridDim.x) {
+    const int64_t items = chunk_off[tv.nleaf];
+    for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
+        // the leaf of item w: chunk_off[lf] <= w < chunk_off[lf + 1] (warp-uniform search)
+        int lo = 0, hi = tv.nleaf;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (chunk_off[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        const int lf = lo;
         const int b = tv.leafbox[lf];
         const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-        const int64_t u0 = tv.u_off[lf], u1 = tv.u_off[lf + 1];
-        for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int64_t u0 = KM == 2 ? tv.s_off[lf] : tv.u_off[lf], u1 = KM == 2 ? tv.s_off[lf + 1] : tv.u_off[lf + 1];
+        if (KM == 2 && u0 == u1) continue;
+        {
+            const int j0 = 32 * (int)(w - chunk_off[lf]);
             const int T = min(32, cnt - j0);
             const int G = near_parts<NU>(T);
             const int U = T * G;
@@ -754,7 +792,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
 #pragma unroll
                 for (int k = 0; k < 4; ++k) ks[r][k] = kc[r][k] = 0.f;
             // round 0: the leaf itself
-            for (int k0 = 0; k0 < cnt; k0 += NEAR_CAP) {
+            for (int k0 = 0; k0 < (KM == 2 ? 0 : cnt); k0 += NEAR_CAP) {
                 const int n = min(NEAR_CAP, cnt - k0);
                 __syncwarp();
                 for (int q = lane; q < n; q += 32) {
@@ -766,7 +804,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                 for (int r = 0; r < R; ++r) {
                     if (!act[r]) continue;
                     float a[4] = {0.f, 0.f, 0.f, 0.f};
-                    p2p_part<true, POT, SOFT>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a, hs, hinv);
+                    p2p_part<true, POT, KM>(s_hi, s_lo, pp[r], G, n, j0 + tt[r] - k0, th[r], tl[r], eps2, a, hs, hinv);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
                         if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);
@@ -778,7 +816,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                 const int64_t e = eb + lane;
                 int pf = 0, pc = 0;
                 if (e < u1) {
-                    const int c = tv.u_idx[e];
+                    const int c = KM == 2 ? tv.s_idx[e] : tv.u_idx[e];
                     if (c != b) { pf = tv.pfirst[c]; pc = tv.pcount[c]; }
                 }
                 int pre = pc;
@@ -813,7 +851,7 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
                     for (int r = 0; r < R; ++r) {
                         if (!act[r]) continue;
                         float a[4] = {0.f, 0.f, 0.f, 0.f};
-                        p2p_part<false, POT, SOFT>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a, hs, hinv);
+                        p2p_part<false, POT, KM>(s_hi, s_lo, pp[r], G, n, -1, th[r], tl[r], eps2, a, hs, hinv);
 #pragma unroll
                         for (int k = 0; k < 4; ++k)
                             if (k < 3 || POT) kahan_add(ks[r][k], kc[r][k], a[k]);
@@ -834,8 +872,14 @@ __global__ void __launch_bounds__(32, 32) k_leaf_near32(TreeView tv, const float
 #pragma unroll
                     for (int k = 0; k < 4; ++k) v[k] += s_red[p * T + lane][k];
                 double2* o = reinterpret_cast<double2*>(near + 4 * (size_t)(f0 + j0 + lane));
-                o[0] = make_double2(v[0], v[1]);
-                o[1] = make_double2(v[2], POT ? v[3] : 0.0);
+                if (KM == 2) {
+                    const double2 o0 = o[0], o1 = o[1];
+                    o[0] = make_double2(o0.x + v[0], o0.y + v[1]);
+                    o[1] = make_double2(o1.x + v[2], o1.y + (POT ? v[3] : 0.0));
+                } else {
+                    o[0] = make_double2(v[0], v[1]);
+                    o[1] = make_double2(v[2], POT ? v[3] : 0.0);
+                }
             }
         }
         __syncwarp();
