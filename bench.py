@@ -173,7 +173,7 @@ def cpu_baseline_single():
 
 # ---------------------------------------------------------------- configs 4 and 5
 SERVE = os.path.join(PKG, "ogx_serve")
-CONFIG4 = ["--ensemble", "--steps", "20", "--jobs", "64", "--nmin", "8192", "--nmax", "262144", "--orders", "6,8",
+CONFIG4 = ["--ensemble", "--steps", "50", "--jobs", "64", "--nmin", "8192", "--nmax", "262144", "--orders", "6,8",
            "--seed", "3"]
 CONFIG5 = ["--jobs", "24", "--rate", "20", "--nmin", "16384", "--nmax", "1048576", "--orders", "6,8,12", "--smin", "10",
            "--smax", "200", "--hbm-gb", "150", "--seed", "1"]
@@ -189,7 +189,7 @@ def serve_run(args, timeout=600):
 
 
 def serving_records():
-    """Config 4 (64 resident systems, N log-uniform 8k-256k, p in {6, 8}, 20 lockstep steps)
+    """Config 4 (64 resident systems, N log-uniform 8k-256k, p in {6, 8}, 50 lockstep steps)
     and config 5 (24 jobs arriving at 20/s, N 16k-1M, p in {6, 8, 12}, 10-200 steps, 150 GB
     budget) through the serving driver, mixed form, eager steps (a job's first steps would pay
     for capturing its step, which these short jobs do not amortise);
@@ -197,8 +197,8 @@ def serving_records():
     FP64 form run one job after another (the comparison config 5 names).  Seeded synthetic
     jobs; wall-clock figures from the driver's own clock."""
     out = {}
-    keep4 = ("bodies_steps_per_s", "ensemble_step_ms_p50", "ensemble_step_ms_p99", "p50_step_ms", "p99_step_ms",
-             "jobs", "failed", "rejected", "graph_launch_steps", "wall_s")
+    keep4 = ("bodies_steps_per_s", "steady_bodies_steps_per_s", "ensemble_step_ms_p50", "ensemble_step_ms_p99",
+             "p50_step_ms", "p99_step_ms", "jobs", "failed", "rejected", "graph_launch_steps", "wall_s")
     keep5 = ("bodies_steps_per_s", "stepping_only_bodies_steps_per_s", "p50_step_ms", "p99_step_ms",
              "job_turnaround_s_p50", "job_turnaround_s_p99", "jobs", "failed", "rejected", "peak_concurrent", "wall_s")
     try:
@@ -263,11 +263,12 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- our arm
-def time_form(ogx, prec, p, pos, vel, mass, device, stream, flush, steps, warmup=2):
+def time_form(ogx, prec, p, pos, vel, mass, device, stream, flush, steps, warmup=2, eps=0.0, softening=0):
     """Step time of one more form on the same workload, measured like the headline (device
     resident, L2 flushed before every step, CUDA events on the library's stream)."""
     import torch
-    with ogx.AdaptiveFMM3D(p=p, threshold=THR, precision=prec, device=device, stream=stream.cuda_stream) as s:
+    with ogx.AdaptiveFMM3D(eps=eps, p=p, threshold=THR, precision=prec, device=device, stream=stream.cuda_stream,
+                           softening=softening) as s:
         s.upload(pos, vel, mass)
         for _ in range(warmup):
             s.step(DT, 1)
@@ -284,7 +285,8 @@ def time_form(ogx, prec, p, pos, vel, mass, device, stream, flush, steps, warmup
     ms = np.array(ms)
     return {"p": p, "ms_per_step": float(ms.mean()), "bodies_per_s": mass.shape[0] / (float(ms.mean()) / 1e3),
             "p50_step_ms": float(np.percentile(ms, 50)), "p99_step_ms": float(np.percentile(ms, 99)),
-            "steps": steps, "ms_m2l": st["ms_m2l"], "ms_leaf": st["ms_leaf"]}
+            "steps": steps, "ms_m2l": st["ms_m2l"], "ms_leaf": st["ms_leaf"], "max_leaf_occupancy": st["max_leaf_occupancy"],
+            "list_s": st["list_s"]}
 
 
 def rms_max(ref, got):
@@ -411,8 +413,15 @@ def main():
                                    "rms_vs_fp64_form": rms_max(a6410, am10)[0]})
         r, m = rms_max(ref, a6410)
         forms["fp64_p10"].update({"rms_vs_fp64_direct": r, "max_rel_vs_fp64_direct": m})
+        # the same merger softened as the reference's own merger run (eps = 0.05): its Plummer
+        # kernel, and the spline kernel with the far field corrected inside its support
+        for kind, name in ((ogx.SOFT_PLUMMER, "mixed_eps0.05_plummer"), (ogx.SOFT_SPLINE, "mixed_eps0.05_spline")):
+            forms[name] = time_form(ogx, ogx.PREC_MIXED, P_ORDER, pos, vel, mass, local, stream, flush, nf, eps=0.05,
+                                    softening=kind)
         forms["note"] = ("same workload and timing as the headline (device-resident leapfrog step, L2 flushed); "
-                         "mixed_speedup = FP64-form step time / mixed-form step time at the same p")
+                         "mixed_speedup = FP64-form step time / mixed-form step time at the same p; "
+                         "mixed_eps0.05_*: the same bodies softened with eps = 0.05 (list_s: leaf pairs the "
+                         "spline's correction covers)")
 
     # ---- roofline of the dominant phase (CUDA events inside the library, same stream)
     phases = {k: float(np.mean([p[k] for p in phase])) for k in

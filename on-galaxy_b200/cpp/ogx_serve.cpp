@@ -649,22 +649,28 @@ int main(int argc, char** argv) {
         }
         stop_pool();
         sampler.finish();
-        double bodysteps = 0.0;
+        double bodysteps = 0.0, bodies = 0.0;
         int failed = 0;
         std::vector<float> all;
         for (const Job& jb : jobs) {
             all.insert(all.end(), jb.step_ms.begin(), jb.step_ms.end());
             bodysteps += (double)jb.n * (double)jb.step_ms.size();
             if (jb.status != OGX_OK && !jb.rejected) ++failed;
+            if (jb.status == OGX_OK && !jb.rejected) bodies += (double)jb.n;
         }
+        // steady state: all resident bodies over the median lockstep step (the first steps of
+        // the one-launch mode step member by member while each member's step is captured)
+        const double p50_ens = percentile(ens_ms, 0.5);
+        const double steady = p50_ens > 0.0 ? bodies / (p50_ens * 1e-3) : 0.0;
         std::printf("{\"mode\": \"ensemble\", \"precision\": \"%s\", \"jobs\": %d, \"failed\": %d, \"rejected\": %d, "
                     "\"steps\": %zu, \"lockstep_steps\": %d, \"workers\": %d, \"wall_s\": %.3f, \"bodies_steps_per_s\": %.6e, "
+                    "\"steady_bodies_steps_per_s\": %.6e, "
                     "\"ensemble_step_ms_p50\": %.3f, \"ensemble_step_ms_p99\": %.3f, \"p50_step_ms\": %.3f, "
                     "\"p99_step_ms\": %.3f, \"peak_concurrent\": %d, \"autotune\": %s, \"warmup_s\": %.3f, "
                     "\"capture\": %s, \"graph\": %s, \"graph_launch_steps\": %lld, \"member_by_member_steps\": %lld, \"member_redos\": %lld, "
                     "\"jobs_detail\": [",
                     precision == OGX_PREC_FP64 ? "fp64" : precision == OGX_PREC_FP64_ROT ? "fp64rot" : "mixed", njobs, failed, rejected, all.size(), S, workers, ens_s,
-                    bodysteps / ens_s, percentile(ens_ms, 0.5), percentile(ens_ms, 0.99), percentile(all, 0.5),
+                    bodysteps / ens_s, steady, p50_ens, percentile(ens_ms, 0.99), percentile(all, 0.5),
                     percentile(all, 0.99), L, autotune ? "true" : "false", warmup_s, g_capture ? "true" : "false", graph ? "true" : "false",
                     (long long)gstats[0], (long long)gstats[1], (long long)gstats[2]);
         for (size_t j = 0; j < jobs.size(); ++j) {

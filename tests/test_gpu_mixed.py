@@ -105,3 +105,23 @@ def test_every_tuning_choice_stays_within_the_mixed_tolerance(ogx, golden, units
         with pytest.raises(ogx.OgxError) as e:
             sm.set_tuning(m2l_tile_targets=48)
         assert e.value.code == ogx.ERR_INVALID
+
+
+@pytest.mark.parametrize("softening", [0, 1])
+def test_mixed_with_leaves_held_large_by_the_eps_floor(ogx, softening):
+    """Disk+bulge galaxy of 100k bodies at eps = 0.05 (the reference's merger setting): the
+    eps floor stops splitting in the bulge, so leaves hold more than the leaf capacity and the near
+    field spreads each over many work items (chunks of 32 targets).  Mixed vs FP64 form,
+    both with Plummer's kernel and with the spline."""
+    from ogx_ic import disk_bulge
+    pos, mass, _ = disk_bulge(100000, seed=4)
+    kw = dict(eps=0.05, p=8, threshold=64, softening=softening)
+    with ogx.AdaptiveFMM3D(precision=ogx.PREC_FP64, **kw) as s64:
+        a64, p64 = s64.compute_accelerations(pos, mass, with_potential=True)
+        st = s64.stats()
+    with ogx.AdaptiveFMM3D(precision=ogx.PREC_MIXED, **kw) as sm:
+        am, pm = sm.compute_accelerations(pos, mass, with_potential=True)
+    assert st["max_leaf_occupancy"] > 64, st["max_leaf_occupancy"]   # above the leaf capacity: the floor acts
+    mx, rms = rel_err(a64, am)
+    assert rms <= 1e-6 and mx <= 1e-3, (mx, rms)
+    assert float(np.sqrt(np.mean((pm - p64) ** 2) / np.mean(p64 ** 2))) <= 1e-6
