@@ -116,6 +116,9 @@ int launch_far32_l2p(Handle& h, const double* L, double* far, bool pot) {
 // operator row (4 where the shared staging fits the 48 KB static limit)
 template <int P>
 constexpr int tr_pb() { return (P + 1) * (P + 1) <= 81 ? 4 : 2; }
+// operator rows in flight per warp (at most ~128 registers, two CTAs per SM)
+template <int P>
+constexpr int tr_kb() { return (P + 1) * (P + 1) <= 96 ? 12 : 6; }
 
 __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     int v;
@@ -213,19 +216,27 @@ __global__ void __launch_bounds__(256) k_translate_flow(TreeView tv, const int* 
         if (any) {  // warp-uniform
             const double* T = opsT + (size_t)s * K * K;
             const int si = MODE == 0 ? s : 0;
-#pragma unroll 8
-            for (int kk = 0; kk < K; ++kk) {
-                double tq[NPL];
+            // operator rows in batches of TR_KB, all loads of a batch issued before its
+            // FMAs (the pass is bound by the chain of L2 round trips); kk order unchanged
+            constexpr int TR_KB = tr_kb<P>();
+            for (int k0 = 0; k0 < K; k0 += TR_KB) {
+                double tq[TR_KB][NPL];
 #pragma unroll
-                for (int q = 0; q < NPL; ++q) {
-                    const int j = lane + 32 * q;
-                    tq[q] = (j < K) ? __ldg(T + (size_t)kk * K + j) : 0.0;
-                }
+                for (int u = 0; u < TR_KB; ++u)
 #pragma unroll
-                for (int a = 0; a < TR_PB; ++a) {
-                    const double v = s_in[si][a][kk];
+                    for (int q = 0; q < NPL; ++q) {
+                        const int j = lane + 32 * q;
+                        tq[u][q] = (k0 + u < K && j < K) ? __ldg(T + (size_t)(k0 + u) * K + j) : 0.0;
+                    }
 #pragma unroll
-                    for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[q], v, acc[a][q]);
+                for (int u = 0; u < TR_KB; ++u) {
+                    if (k0 + u >= K) break;
+#pragma unroll
+                    for (int a = 0; a < TR_PB; ++a) {
+                        const double v = s_in[si][a][k0 + u];
+#pragma unroll
+                        for (int q = 0; q < NPL; ++q) acc[a][q] = fma(tq[u][q], v, acc[a][q]);
+                    }
                 }
             }
         }
@@ -416,15 +427,33 @@ __global__ void __launch_bounds__(M2L_THREADS) k_m2l_fp64(TreeView tv, const uin
 }
 
 // ---- leaf near field (P2P over U) + final combine ----------------------------------------
+// the leaf and first target of near-field work item w (leaf, chunk of 32 targets):
+// chunk_off[lf] <= w < chunk_off[lf + 1]; false past the last item
+__device__ __forceinline__ bool near_item(const TreeView& tv, const int64_t* chunk_off, int64_t w, int& lf, int& j0) {
+    if (w >= chunk_off[tv.nleaf]) return false;
+    int lo = 0, hi = tv.nleaf;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (chunk_off[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    lf = lo;
+    j0 = 32 * (int)(w - chunk_off[lo]);
+    return true;
+}
+
+// Warp per work item (leaf, chunk of 32 targets), so a leaf held large by the eps floor
+// spreads over many warps.
 template <bool POT, bool SOFT = false>
-__global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double eps2, const double* far, double* acc, double* pot,
-                                                   double hs = 0.0, double hinv = 0.0) {
+__global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, const int64_t* __restrict__ chunk_off, double G, double eps2,
+                                                   const double* far, double* acc, double* pot, double hs = 0.0,
+                                                   double hinv = 0.0) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int lf = blockIdx.x * 4 + wid;
-    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
+    int lf, j0;
+    if (tv_over(tv) || !near_item(tv, chunk_off, blockIdx.x * 4 + wid, lf, j0)) return;
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
-    for (int j0 = 0; j0 < cnt; j0 += 32) {
+    {
         const int jj = j0 + lane;
         const bool act = jj < cnt;
         const int i = f0 + (act ? jj : 0);
@@ -474,16 +503,17 @@ __global__ void __launch_bounds__(128) k_leaf_near(TreeView tv, double G, double
 // Warp per leaf, lanes over the leaf's bodies, FP64 (the plain form; the mixed form runs
 // the FP32 near-field kernel over the same lists, mixed::k_leaf_near32<.., 2>).
 template <bool POT>
-__global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, double hs, double hinv, double* out) {
+__global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, const int64_t* __restrict__ chunk_off, double hs, double hinv,
+                                                      double* out) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int lf = blockIdx.x * 4 + wid;
-    if (lf >= tv.nleaf || lf >= tv_nleaf(tv) || tv_over(tv)) return;
+    int lf, j0;
+    if (tv_over(tv) || !near_item(tv, chunk_off, blockIdx.x * 4 + wid, lf, j0)) return;
     const int64_t e0 = tv.s_off[lf], e1 = tv.s_off[lf + 1];
     if (e0 == e1) return;
     const int b = tv.leafbox[lf];
     const int f0 = tv.pfirst[b], cnt = tv.pcount[b];
     const double hs2 = hs * hs;
-    for (int j0 = 0; j0 < cnt; j0 += 32) {
+    {
         const int jj = j0 + lane;
         const bool act = jj < cnt;
         const int i = f0 + (act ? jj : 0);
@@ -517,12 +547,24 @@ __global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, double hs, do
 
 }  // namespace
 
-int soft_correct_launch(Handle& h, double* out, bool pot, cudaStream_t st) {
+// work items of the near field (leaf, chunk of 32 targets), on h.stream; the grid of a
+// warp-per-item kernel needs at most nleaf + n / 32 warps
+int near_items(Handle& h, int64_t** chunk_off) {
+    TreeView& tv = h.tv;
+    int* nchunk;
+    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK, (size_t)tv.nleaf, &nchunk));
+    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK_OFF, (size_t)tv.nleaf + 1, chunk_off));
+    mixed::k_near_chunks<<<(tv.nleaf + 255) / 256, 256, 0, h.stream>>>(tv, nchunk); ++h.launches;
+    return scan_i32_to_i64(h, nchunk, *chunk_off, tv.nleaf);
+}
+
+int soft_correct_launch(Handle& h, const int64_t* chunk_off, double* out, bool pot, cudaStream_t st) {
     const TreeView& tv = h.tv;
     if (h.soft_pairs == 0 || tv.nleaf == 0) return OGX_OK;
     const double hs = spline_support(h.prm.eps), hinv = 1.0 / hs;
-    if (pot) k_soft_correct<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hs, hinv, out);
-    else k_soft_correct<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, hs, hinv, out);
+    const int grid = (tv.nleaf + (tv.n + 31) / 32 + 3) / 4;
+    if (pot) k_soft_correct<true><<<grid, 128, 0, st>>>(tv, chunk_off, hs, hinv, out);
+    else k_soft_correct<false><<<grid, 128, 0, st>>>(tv, chunk_off, hs, hinv, out);
     ++h.launches;
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
@@ -573,15 +615,18 @@ int run_fp64(Handle& h, double* d_acc, double* d_pot) {
     const bool pot = d_pot != nullptr;
     OGX_TRY((launch_far<P, double>(h, M, L, far, pot)));
     const double G = h.prm.G, eps2 = h.prm.eps * h.prm.eps;
+    int64_t* chunk_off;
+    OGX_TRY(near_items(h, &chunk_off));
+    const int ngrid = (tv.nleaf + (tv.n + 31) / 32 + 3) / 4;   // a warp per work item
     if (h.prm.softening == OGX_SOFT_SPLINE) {
         // the far field's pairs within the support, then the spline kernel in the near field
-        OGX_TRY(soft_correct_launch(h, far, pot, st));
+        OGX_TRY(soft_correct_launch(h, chunk_off, far, pot, st));
         const double hs = spline_support(h.prm.eps), hinv = hs > 0.0 ? 1.0 / hs : 0.0;
-        if (pot) k_leaf_near<true, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot, hs, hinv);
-        else k_leaf_near<false, true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr, hs, hinv);
+        if (pot) k_leaf_near<true, true><<<ngrid, 128, 0, st>>>(tv, chunk_off, G, eps2, far, d_acc, d_pot, hs, hinv);
+        else k_leaf_near<false, true><<<ngrid, 128, 0, st>>>(tv, chunk_off, G, eps2, far, d_acc, nullptr, hs, hinv);
         ++h.launches;
-    } else if (pot) { k_leaf_near<true><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, d_pot); ++h.launches; }
-    else { k_leaf_near<false><<<(tv.nleaf + 3) / 4, 128, 0, st>>>(tv, G, eps2, far, d_acc, nullptr); ++h.launches; }
+    } else if (pot) { k_leaf_near<true><<<ngrid, 128, 0, st>>>(tv, chunk_off, G, eps2, far, d_acc, d_pot); ++h.launches; }
+    else { k_leaf_near<false><<<ngrid, 128, 0, st>>>(tv, chunk_off, G, eps2, far, d_acc, nullptr); ++h.launches; }
     OGX_CUDA(timing_record(h, h.ev[7], st));
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
@@ -771,13 +816,9 @@ int run_mixed(Handle& h, double* d_acc, double* d_pot) {
     OGX_TRY(arena_get(h.ws, S_FAR_M, 4 * (size_t)tv.n, &far_m));
     const size_t p2x_smem = p2x_smem_bytes<P, float>();
     OGX_CUDA(smem_optin((const void*)k_p2x<P, 1, float>, (int)p2x_smem));
-    // near-field work items (leaf, chunk of 32 targets): counts and offsets
-    int* nchunk;
+    // near-field work items (leaf, chunk of 32 targets)
     int64_t* chunk_off;
-    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK, (size_t)tv.nleaf, &nchunk));
-    OGX_TRY(arena_get(h.ws, S_NEAR_CHUNK_OFF, (size_t)tv.nleaf + 1, &chunk_off));
-    mixed::k_near_chunks<<<(tv.nleaf + 255) / 256, 256, 0, st>>>(tv, nchunk); ++h.launches;
-    OGX_TRY(scan_i32_to_i64(h, nchunk, chunk_off, tv.nleaf));
+    OGX_TRY(near_items(h, &chunk_off));
     // join the upward pass (the side stream's M2P reads the multipoles)
     OGX_CUDA(cudaStreamWaitEvent(st, h.ev_up, 0));
     // the far field's M2P part and the near field need the tree, the multipoles and the

@@ -313,7 +313,7 @@ int lists_build(Handle& h);           // both parts below, in order
 int lists_build_targets(Handle& h);   // colleagues; M2L target tiles on `aux`
 int lists_build_uwx(Handle& h);       // U, W and X lists
 int soft_lists_build(Handle& h);      // OGX_SOFT_SPLINE: the leaf pairs the far field takes within the support
-int soft_correct_launch(Handle& h, double* out, bool pot, cudaStream_t st);   // adds the kernel difference over them
+int soft_correct_launch(Handle& h, const int64_t* chunk_off, double* out, bool pot, cudaStream_t st);   // FP64: adds the kernel difference over them
 int fmm_fp64(Handle& h, double* d_acc, double* d_pot);
 int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int m2l_rot_launch(Handle& h, const double* M, double* Lown);   // third form's M2L, on h.stream
