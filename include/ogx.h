@@ -99,6 +99,7 @@ typedef struct {
     int64_t graph_steps;       /* ogx_step calls' steps replayed from a captured graph (running total) */
     int64_t step_redos;        /* steps redone eagerly after a capacity overflow (running total) */
     int64_t list_s;            /* OGX_SOFT_SPLINE: (leaf, leaf) pairs the far field takes within the support */
+    int64_t graph_evals;       /* ogx_eval calls replayed from a captured graph (running total) */
 } ogx_stats;
 
 /* Fill *prm with defaults: G=1, eps=0, p=8, leaf_capacity=64, adaptive FMM, FP64, device 0,
@@ -166,6 +167,11 @@ const char* ogx_strerror(int status);
  *                      results are those of eager steps.  Each step ends with a host sync.
  *                      A handle whose stream is the legacy or per-thread default stream
  *                      steps eagerly (capture is not possible there).
+ *                      ogx_eval on page-locked host buffers works the same way: the call
+ *                      after the capacities were set runs uncaptured, the next records
+ *                      copies in, evaluation and copies out as one graph, and later calls
+ *                      with the same n and buffers replay it (other buffers start over).
+ *                      Steps and such evaluations of OGX_SOFT_SPLINE handles stay eager.
  * ogx_set_tuning applies from the next evaluation on; 0 in a size field keeps its default. */
 typedef struct {
     int m2l_tile_targets;

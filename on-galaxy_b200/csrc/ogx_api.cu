@@ -321,6 +321,12 @@ void drop_step_graph(Handle& h) {
     h.step_exec = nullptr;
     h.step_graph = nullptr;
     h.cap_warm = 0;
+    // the captured host-buffer evaluation is released on the same occasions
+    if (h.eval_exec) cudaGraphExecDestroy(h.eval_exec);
+    if (h.eval_graph) cudaGraphDestroy(h.eval_graph);
+    h.eval_exec = nullptr;
+    h.eval_graph = nullptr;
+    h.eval_warm = 0;
 }
 
 // Record one step in capacity mode as a CUDA graph (nothing is launched).
@@ -614,6 +620,8 @@ int ogx_create(const ogx_params* prm, void** handle) {
     OGX_CUDA(cudaEventCreateWithFlags(&h->ev_col, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreateWithFlags(&h->ev_tgt, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreateWithFlags(&h->ev_m2l, cudaEventDisableTiming));
+    OGX_CUDA(cudaEventCreateWithFlags(&h->ev_mass, cudaEventDisableTiming));
+    OGX_CUDA(cudaEventCreateWithFlags(&h->ev_pos, cudaEventDisableTiming));
     for (cudaEvent_t* e : {&h->ev_fork, &h->ev_join, &h->ev_in, &h->ev_out, &h->ev_tree, &h->ev_up})
         OGX_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     OGX_CUDA(cudaEventCreate(&h->ev_up_end));
@@ -634,7 +642,7 @@ int ogx_destroy(void* handle) {
         if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto& e : h->ev)
             if (e) cudaEventDestroy(e);
-        for (cudaEvent_t e : {h->ev_col, h->ev_tgt, h->ev_m2l})
+        for (cudaEvent_t e : {h->ev_col, h->ev_tgt, h->ev_m2l, h->ev_mass, h->ev_pos})
             if (e) cudaEventDestroy(e);
         for (cudaStream_t sx : {h->main, h->side, h->up, h->aux, h->m2l})
             if (sx) {
@@ -675,6 +683,92 @@ int ogx_synchronize(void* handle) {
     return OGX_OK;
 }
 
+// Copies in, evaluation, copies out of one host-buffer evaluation, issued on h.stream
+// (eagerly, in capacity mode, or into a capture); timing events: h2d ev[10]..ev[11],
+// d2h ev[12]..ev[13].
+static int eval_host_issue(Handle& h, int64_t n, const double* pos, const double* mass, double* acc, double* pot,
+                           double* dp, double* dm, double* da, double* dpot) {
+    OGX_CUDA(timing_record(h, h.ev[10], h.stream));
+    OGX_CUDA(cudaMemcpyAsync(dp, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+    // the masses are first read at the end of the tree build (the sorted-body gather), so
+    // their copy runs on the aux stream beside the bounding box, keys and sort
+    const bool fmm = h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM;
+    if (fmm) {
+        // after the positions (the two copies would otherwise share the link and the
+        // positions, which the tree build needs first, would arrive no earlier)
+        OGX_CUDA(cudaEventRecord(h.ev_pos, h.stream));
+        OGX_CUDA(cudaStreamWaitEvent(h.aux, h.ev_pos, 0));
+        OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.aux));
+        OGX_CUDA(cudaEventRecord(h.ev_mass, h.aux));
+        OGX_CUDA(timing_record(h, h.ev[11], h.aux));
+        h.mass_pending = true;
+    } else {
+        OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+        OGX_CUDA(timing_record(h, h.ev[11], h.stream));
+    }
+    const int rc_eval = eval_device(h, n, dp, dm, da, dpot);
+    if (h.mass_pending) {   // an evaluation that stopped before the gather still orders the copy
+        cudaStreamWaitEvent(h.stream, h.ev_mass, 0);
+        h.mass_pending = false;
+    }
+    OGX_TRY(rc_eval);
+    OGX_CUDA(timing_record(h, h.ev[12], h.stream));
+    OGX_CUDA(cudaMemcpyAsync(acc, da, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    if (pot) OGX_CUDA(cudaMemcpyAsync(pot, dpot, n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    OGX_CUDA(timing_record(h, h.ev[13], h.stream));
+    return OGX_OK;
+}
+
+static bool page_locked(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Record one host-buffer evaluation in capacity mode as a CUDA graph (nothing runs).
+static int capture_eval(Handle& h, int64_t n, const double* pos, const double* mass, double* acc, double* pot, double* dp,
+                        double* dm, double* da, double* dpot) {
+    const int64_t l0 = h.launches;
+    OGX_CUDA(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeRelaxed));
+    h.capturing = true;
+    h.cap_mode = true;
+    h.ws.frozen = true;
+    const int rc = eval_host_issue(h, n, pos, mass, acc, pot, dp, dm, da, dpot);
+    h.ws.frozen = false;
+    h.cap_mode = false;
+    h.capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(h.stream, &g);
+    if (rc != OGX_OK || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (rc != OGX_OK) return rc;
+        set_last_error(OGX_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ec));
+        return OGX_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiateWithFlags(&h.eval_exec, g, cudaGraphInstantiateFlagUseNodePriority);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        h.eval_exec = nullptr;
+        set_last_error(OGX_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+        return OGX_ERR_CUDA;
+    }
+    h.eval_graph = g;
+    h.eval_launches = h.launches - l0;
+    h.eval_gen = h.ws.generation;
+    return OGX_OK;
+}
+
+// ForceSolver3D::computeAccelerations on host buffers.  Eager by default.  With step
+// capture on (ogx_set_tuning), page-locked buffers and an adaptive-FMM handle with
+// Plummer softening, the first call after the capacities were set runs uncaptured in
+// capacity mode, the next is recorded as a CUDA graph (copies in, evaluation, copies
+// out) and later calls with the same n and buffers replay it; a call that outgrew its
+// capacities is redone eagerly, which sets new ones.  Results equal eager calls.
 int ogx_eval(void* handle, int64_t n, const double* pos, const double* mass, double* acc, double* pot) {
     if (!handle || n < 0 || n > (int64_t)INT32_MAX / 2) return OGX_ERR_INVALID;
     if (n > 0 && (!pos || !mass || !acc)) return OGX_ERR_INVALID;
@@ -689,22 +783,61 @@ int ogx_eval(void* handle, int64_t n, const double* pos, const double* mass, dou
     OGX_TRY(arena_get(h.ws, S_MASS, n, &dm));
     OGX_TRY(arena_get(h.ws, S_ACC, 3 * n, &da));
     if (pot) OGX_TRY(arena_get(h.ws, S_POT, n, &dpot));
-    cudaEvent_t e0 = h.ev[10], e1 = h.ev[11];
-    OGX_CUDA(cudaEventRecord(e0, h.stream));
-    OGX_CUDA(cudaMemcpyAsync(dp, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-    OGX_CUDA(cudaMemcpyAsync(dm, mass, n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-    OGX_CUDA(cudaEventRecord(e1, h.stream));
-    OGX_TRY(eval_device(h, n, dp, dm, da, dpot));
-    const float h2d = (cudaEventSynchronize(e1) == cudaSuccess) ? ev_ms(e0, e1) : 0.f;
-    OGX_CUDA(cudaEventRecord(e0, h.stream));
-    OGX_CUDA(cudaMemcpyAsync(acc, da, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
-    if (pot) OGX_CUDA(cudaMemcpyAsync(pot, dpot, n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
-    OGX_CUDA(cudaEventRecord(e1, h.stream));
+    const bool capturable = h.stream != nullptr && h.stream != cudaStreamLegacy && h.stream != cudaStreamPerThread;
+    const bool graphed = h.capture_steps && capturable && h.prm.solver == OGX_SOLVER_ADAPTIVE_FMM && h.cap.valid &&
+                         h.prm.softening == OGX_SOFT_PLUMMER && page_locked(pos) && page_locked(mass) &&
+                         page_locked(acc) && page_locked(pot);
+    int64_t launched = 0;
+    if (!graphed) {
+        h.cap_mode = false;
+        OGX_TRY(eval_host_issue(h, n, pos, mass, acc, pot, dp, dm, da, dpot));
+    } else {
+        Handle::EvalKey key;
+        key.n = n; key.pos = pos; key.mass = mass; key.acc = acc; key.pot = pot;
+        if (h.eval_exec && (!(key == h.eval_key) || h.eval_gen != h.ws.generation)) {
+            if (h.eval_exec) cudaGraphExecDestroy(h.eval_exec);
+            if (h.eval_graph) cudaGraphDestroy(h.eval_graph);
+            h.eval_exec = nullptr;
+            h.eval_graph = nullptr;
+            h.eval_warm = 0;
+        }
+        if (h.eval_exec) {
+            OGX_CUDA(cudaGraphLaunch(h.eval_exec, h.stream));
+            h.launches += h.eval_launches;
+            launched = h.eval_launches;
+            ++h.graph_evals;
+        } else if (h.eval_warm == 0 || !(key == h.eval_key)) {
+            const int64_t l0 = h.launches;
+            h.cap_mode = true;
+            const int rc = eval_host_issue(h, n, pos, mass, acc, pot, dp, dm, da, dpot);
+            h.cap_mode = false;
+            OGX_TRY(rc);
+            h.eval_warm = 1;
+            h.eval_key = key;
+            launched = h.launches - l0;
+        } else {
+            OGX_TRY(capture_eval(h, n, pos, mass, acc, pot, dp, dm, da, dpot));
+            OGX_CUDA(cudaGraphLaunch(h.eval_exec, h.stream));
+            launched = h.eval_launches;
+            ++h.graph_evals;
+        }
+    }
     OGX_CUDA(cudaStreamSynchronize(h.stream));
     OGX_TRY(device_error(h));
+    if (graphed && h.h_counts->overflow) {
+        // the tree or the lists outgrew the capacities: redo eagerly (new capacities)
+        drop_step_graph(h);
+        h.cap_mode = false;
+        OGX_TRY(eval_host_issue(h, n, pos, mass, acc, pot, dp, dm, da, dpot));
+        OGX_CUDA(cudaStreamSynchronize(h.stream));
+        OGX_TRY(device_error(h));
+        ++h.overflow_redos;
+        launched = 0;
+    }
     finish_stats(h);
-    h.stats.ms_h2d = h2d;
-    h.stats.ms_d2h = ev_ms(e0, e1);
+    if (launched) h.stats.launches = launched;
+    h.stats.ms_h2d = ev_ms(h.ev[10], h.ev[11]);
+    h.stats.ms_d2h = ev_ms(h.ev[12], h.ev[13]);
     return OGX_OK;
 }
 
@@ -715,6 +848,7 @@ int ogx_last_stats(void* handle, ogx_stats* out) {
     if (h.stats.ms_total == 0.0) finish_stats(h);
     h.stats.graph_steps = h.graph_steps;
     h.stats.step_redos = h.overflow_redos;
+    h.stats.graph_evals = h.graph_evals;
     *out = h.stats;
     return OGX_OK;
 }

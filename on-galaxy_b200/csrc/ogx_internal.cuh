@@ -233,7 +233,7 @@ struct Handle {
     // device-resident integrator state
     bool resident = false;
     bool species_set = false;       // species tags uploaded (or made by ogx_ic_merger)
-    cudaEvent_t ev[12] = {};
+    cudaEvent_t ev[14] = {};
     // side stream for work that overlaps the main chain (joined back before returning)
     // internal streams: the evaluation runs on `main` (highest priority), forked
     // from and joined back to the caller's stream; overlapping work goes to `side`
@@ -244,6 +244,10 @@ struct Handle {
     // target tiles are ready, beside the rest of the list build
     cudaStream_t m2l = nullptr;
     cudaEvent_t ev_col = nullptr, ev_tgt = nullptr, ev_m2l = nullptr;
+    // host-buffer evaluation: the masses' copy runs on `aux` beside the start of the tree
+    // build, which waits for it (ev_mass) before the sorted-body gather
+    cudaEvent_t ev_mass = nullptr, ev_pos = nullptr;
+    bool mass_pending = false;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_in = nullptr, ev_out = nullptr, ev_tree = nullptr, ev_up = nullptr;
     cudaEvent_t ev_up_end = nullptr;   // timing: end of an upward pass that ran on `up`
     bool upward_split = false;         // the last evaluation ran its upward pass on `up`
@@ -272,6 +276,23 @@ struct Handle {
     uint64_t step_gen = 0;        // arena generation the captured step was recorded with
     int64_t overflow_redos = 0;   // steps redone eagerly after an overflow
     int64_t graph_steps = 0;      // steps replayed from the captured graph
+    // the captured host-buffer evaluation (ogx_eval with step capture on and page-locked
+    // buffers): copies in, evaluation, copies out, for the buffers it was captured with
+    struct EvalKey {
+        int64_t n = -1;
+        const void *pos = nullptr, *mass = nullptr;
+        void *acc = nullptr, *pot = nullptr;
+        bool operator==(const EvalKey& o) const {
+            return n == o.n && pos == o.pos && mass == o.mass && acc == o.acc && pot == o.pot;
+        }
+    };
+    cudaGraph_t eval_graph = nullptr;
+    cudaGraphExec_t eval_exec = nullptr;
+    EvalKey eval_key;
+    uint64_t eval_gen = 0;
+    int eval_warm = 0;
+    int64_t eval_launches = 0;
+    int64_t graph_evals = 0;      // host-buffer evaluations replayed from the captured graph
     DevCounts* d_counts = nullptr;   // the counts of the last evaluation (device)
     int* d_level_off = nullptr;      // first box of every level (device, kMaxDepth + 2)
     // launch-shape knobs (ogx_set_tuning)

@@ -521,6 +521,10 @@ int tree_build(Handle& h, const double* d_pos, const double* d_mass, int64_t n) 
     OGX_TRY(arena_get(h.ws, S_PY, n, &py));
     OGX_TRY(arena_get(h.ws, S_PZ, n, &pz));
     OGX_TRY(arena_get(h.ws, S_PM, n, &pm));
+    if (h.mass_pending) {   // the masses' host copy (ogx_eval) ran beside the steps above
+        OGX_CUDA(cudaStreamWaitEvent(st, h.ev_mass, 0));
+        h.mass_pending = false;
+    }
     k_gather_bodies<<<grid_for(n, 256), 256, 0, st>>>(perm_s, d_pos, d_mass, n, perm, px, py, pz, pm); ++h.launches;
     OGX_CUDA(cudaGetLastError());
 

@@ -53,7 +53,8 @@ class Stats(C.Structure):
                 ("ms_tree", C.c_double), ("ms_lists", C.c_double), ("ms_upward", C.c_double), ("ms_m2l", C.c_double),
                 ("ms_p2l", C.c_double), ("ms_downward", C.c_double), ("ms_leaf", C.c_double), ("ms_total", C.c_double),
                 ("ms_h2d", C.c_double), ("ms_d2h", C.c_double), ("launches", C.c_int64),
-                ("graph_steps", C.c_int64), ("step_redos", C.c_int64), ("list_s", C.c_int64)]
+                ("graph_steps", C.c_int64), ("step_redos", C.c_int64), ("list_s", C.c_int64),
+                ("graph_evals", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
