@@ -18,6 +18,9 @@
 // starts step s + 1), their steps spread over the same worker pool; the line then also
 // carries the lockstep step time (p50 / p99).
 //
+// --eps E --softening plummer|spline: every job's softening (default: eps 0, Plummer's
+// kernel as the reference; spline = compact kernel with the far field corrected inside
+// its support, whose steps stay eager);
 // --capture: every job's steps replay a CUDA graph of its step (ogx_tuning.capture_steps);
 // the results are bit-identical to eager steps.
 // --graph (with --ensemble): the systems advance through ogx_ensemble_step, every lockstep
@@ -145,6 +148,8 @@ double footprint_bytes(int64_t n, int p) {
 }
 
 bool g_capture = false;   // --capture: every job replays its captured step (ogx_tuning.capture_steps)
+double g_eps = 0.0;       // --eps: softening length of every job
+int g_softening = OGX_SOFT_PLUMMER;   // --softening plummer|spline
 
 // create the job's handle and its initial conditions on the device
 void* open_job(Job& job, int precision) {
@@ -153,6 +158,8 @@ void* open_job(Job& job, int precision) {
     prm.p = job.p;
     prm.leaf_capacity = job.thr;
     prm.precision = precision;
+    prm.eps = g_eps;
+    prm.softening = g_softening;
     void* h = nullptr;
     if ((job.status = ogx_create(&prm, &h)) != OGX_OK) return nullptr;
     ogx_tuning tu{job.fill, job.units, g_capture ? 1 : 0};
@@ -396,6 +403,16 @@ int main(int argc, char** argv) {
         else if (a == "--autotune") autotune = true;
         else if (a == "--graph") graph = true;
         else if (a == "--capture") g_capture = true;
+        else if (a == "--eps") g_eps = std::atof(next().c_str());
+        else if (a == "--softening") {
+            const std::string v = next();
+            if (v == "plummer") g_softening = OGX_SOFT_PLUMMER;
+            else if (v == "spline") g_softening = OGX_SOFT_SPLINE;
+            else {
+                std::fprintf(stderr, "unknown softening '%s' (expected plummer or spline)\n", v.c_str());
+                return 2;
+            }
+        }
         else if (a == "--tune-cache") tune_cache = next();
         else if (a == "--thr") thr = std::atoi(next().c_str());
         else if (a == "--workers") workers = std::atoi(next().c_str());

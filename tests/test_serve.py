@@ -96,6 +96,28 @@ def test_fp64_jobs_give_the_same_bits_alone_and_in_the_mix():
     assert [j["digest"] for j in solo["jobs_detail"]] == [j["digest"] for j in mixed["jobs_detail"]]
 
 
+@pytest.mark.gpu
+def test_softened_jobs_give_the_same_bits_alone_and_in_the_mix():
+    """Jobs with eps = 0.05 and the spline kernel (far field corrected inside its support):
+    the same bits alone and in the mix, and different bits from the Plummer kernel."""
+    args = ("--jobs", 4, "--rate", 400, "--nmin", 16384, "--nmax", 65536, "--smin", 2, "--smax", 4,
+            "--orders", "6,8", "--seed", 13, "--eps", 0.05)
+    solo = _serve(*args, "--softening", "spline", "--solo")
+    mixed = _serve(*args, "--softening", "spline")
+    plummer = _serve(*args, "--solo")
+    assert solo["failed"] == mixed["failed"] == plummer["failed"] == 0
+    digests = [j["digest"] for j in solo["jobs_detail"]]
+    assert digests == [j["digest"] for j in mixed["jobs_detail"]]
+    assert all(a != b for a, b in zip(digests, [j["digest"] for j in plummer["jobs_detail"]]))
+
+
+def test_serve_rejects_an_unknown_softening():
+    if not os.path.exists(SERVE):
+        pytest.skip("ogx_serve not built")
+    r = subprocess.run([SERVE, "--softening", "gaussian"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+
+
 ENS = ("--ensemble", "--steps", 4, "--jobs", 12, "--nmin", 8192, "--nmax", 131072, "--orders", "6,8", "--seed", 5)
 
 
