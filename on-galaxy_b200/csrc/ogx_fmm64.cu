@@ -142,7 +142,7 @@ __device__ bool wait_ready(const int* flag, int* err) {
 
 template <int P, int MODE>
 __global__ void __launch_bounds__(256) k_translate_flow(TreeView tv, const int* __restrict__ nonleaf,
-                                                        const int* __restrict__ nl_off, int nlev,
+                                                        const int* __restrict__ nl_off, int nlev, int ibeg, int iend,
                                                         const double* __restrict__ opsT, double* mpole, double* local,
                                                         const double* __restrict__ lown, int* ready, int* ticket,
                                                         int* err) {
@@ -154,10 +154,10 @@ __global__ void __launch_bounds__(256) k_translate_flow(TreeView tv, const int* 
     __shared__ int s_gend[kMaxDepth + 2];   // groups of the pass's first i+1 levels
     __shared__ int s_t;
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
-    if (tv_over(tv) || nlev <= 0) return;
+    if (tv_over(tv) || nlev <= 0 || ibeg >= iend) return;
     if (threadIdx.x == 0) {
         int c = 0;
-        for (int i = 0; i < nlev; ++i) {
+        for (int i = 0; i < iend; ++i) {
             const int l = MODE == 1 ? i : nlev - 1 - i;
             c += (nl_off[l + 1] - nl_off[l] + TR_PB - 1) / TR_PB;
             s_gend[i] = c;
@@ -165,10 +165,12 @@ __global__ void __launch_bounds__(256) k_translate_flow(TreeView tv, const int* 
     }
     for (;;) {
         __syncthreads();   // s_gend is written; the previous group's shared data was read
-        if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1);
+        // this launch's levels are pass-order indices [ibeg, iend): its tickets count from
+        // the first group of level ibeg
+        if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1) + (ibeg > 0 ? s_gend[ibeg - 1] : 0);
         __syncthreads();
         const int t = s_t;
-        if (t >= s_gend[nlev - 1]) break;
+        if (t >= s_gend[iend - 1]) break;
         int i = 0;
         while (t >= s_gend[i]) ++i;
         const int l = MODE == 1 ? i : nlev - 1 - i;
@@ -298,8 +300,13 @@ int translate_groups(const Handle& h, int l) {
     return (nbl + tr_pb<P>() - 1) / tr_pb<P>();
 }
 
-// one launch of a translation pass: CTAs for every SM (as many as fit), at most one per
-// group; the ready flags and the ticket counter are cleared first
+// A translation pass.  A tree of at least kFlowBoxes boxes takes one launch over every
+// level: CTAs for every SM (as many as fit), at most one per group.  A smaller tree (a
+// system that shares the GPU with others, typically) takes one launch per level, each
+// with its level's groups only: its level chain would otherwise keep waiting CTAs on
+// most SMs while its few groups per level run.  Same kernel, same arithmetic per box.
+// The ready flags and the ticket counters (one per launch) are cleared first.
+constexpr int kFlowBoxes = 32768;
 template <int P, int MODE>
 int launch_translate(Handle& h, Slot slot, double* M, double* L, const double* Lown) {
     const int nlev = h.max_level;   // parent levels 0 .. max_level-1
@@ -316,13 +323,25 @@ int launch_translate(Handle& h, Slot slot, double* M, double* L, const double* L
         return std::max(1, b);
     }();
     int* ready;
-    OGX_TRY(arena_get(h.ws, slot, (size_t)h.tv.nb + 1, &ready));
-    OGX_CUDA(cudaMemsetAsync(ready, 0, sizeof(int) * ((size_t)h.tv.nb + 1), h.stream));
-    const int grid = std::min(groups, per_sm * h.num_sms);
-    k_translate_flow<P, MODE><<<grid, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, nlev,
-                                                          MODE == 0 ? h.d_m2m : h.d_l2l, M, L, Lown, ready,
-                                                          ready + h.tv.nb, h.d_err);
-    ++h.launches;
+    const size_t nready = (size_t)h.tv.nb + kMaxDepth + 2;
+    OGX_TRY(arena_get(h.ws, slot, nready, &ready));
+    OGX_CUDA(cudaMemsetAsync(ready, 0, sizeof(int) * nready, h.stream));
+    int* tickets = ready + h.tv.nb;
+    const double* ops = MODE == 0 ? h.d_m2m : h.d_l2l;
+    if (h.tv.nb >= kFlowBoxes) {
+        const int grid = std::min(groups, per_sm * h.num_sms);
+        k_translate_flow<P, MODE><<<grid, 256, 0, h.stream>>>(h.tv, h.d_nonleaf, h.d_nonleaf_off, nlev, 0, nlev, ops, M, L,
+                                                              Lown, ready, tickets, h.d_err);
+        ++h.launches;
+    } else {
+        for (int i = 0; i < nlev; ++i) {
+            const int g = translate_groups<P>(h, MODE == 1 ? i : nlev - 1 - i);
+            if (g <= 0) continue;
+            k_translate_flow<P, MODE><<<std::min(g, per_sm * h.num_sms), 256, 0, h.stream>>>(
+                h.tv, h.d_nonleaf, h.d_nonleaf_off, nlev, i, i + 1, ops, M, L, Lown, ready, tickets + i, h.d_err);
+            ++h.launches;
+        }
+    }
     OGX_CUDA(cudaGetLastError());
     return OGX_OK;
 }
