@@ -76,6 +76,19 @@ def test_galaxy_262k_fp64_form_matches_oracle(ogx, oracle, galaxy262k, p):
     assert mx <= FMM_TOL, (p, mx, rms)
 
 
+def test_galaxy_262k_fp64_form_one_launch_translations_match_oracle(ogx, oracle, galaxy262k):
+    """Leaf capacity 16: about 63k boxes, so M2M and L2L each run as one launch over all
+    levels (groups of parents taken by ticket, waiting on per-box ready flags) instead of
+    one launch per level; the FP64 form still equals the oracle to 1e-12."""
+    pos, mass = galaxy262k
+    with ogx.AdaptiveFMM3D(p=4, threshold=16, precision=ogx.PREC_FP64) as s:
+        acc = s.compute_accelerations(pos, mass)
+        assert s.stats()["num_boxes"] >= 32768
+    ref = oracle.adaptive_fmm(pos, mass, p=4, thr=16, with_pot=False)
+    mx, rms = rel_err(ref, acc)
+    assert mx <= FMM_TOL, (mx, rms)
+
+
 def test_merger_1m_direct_sum_matches_cpu_on_seeded_targets(ogx, oracle, merger1m):
     pos, mass = merger1m
     with ogx.DirectSolver3D() as d:
