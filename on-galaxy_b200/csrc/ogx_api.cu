@@ -10,11 +10,13 @@
 // Errors are status codes; nothing throws or exits across the boundary
 // (the reference exit()s on CUDA errors, src3d/gpu/AdaptiveFMM3DGPU.cu:23-26).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 
 #include "ogx_harmonics.cuh"
 #include "ogx_sm100.cuh"
@@ -507,7 +509,38 @@ static int build_ensemble_graph(Ensemble& e) {
 int ensemble_step(Ensemble& e, double dt) {
     if (!ensemble_current(e)) {
         drop_ensemble_graph(e);
-        for (Handle* h : e.members) OGX_TRY(step_member(*h, dt));
+        // the members' own steps (uncaptured warm-up, then capture) are independent, so a
+        // few host threads take them; each handle is driven by one thread at a time
+        const int nm = (int)e.members.size();
+        const int nt = std::min(nm, 8);
+        std::atomic<int> next{0};
+        std::mutex mu;
+        int rc_first = OGX_OK;
+        std::string msg;
+        auto work = [&]() {
+            for (;;) {
+                const int i = next.fetch_add(1);
+                if (i >= nm) return;
+                Handle& m = *e.members[i];
+                DeviceGuard g(m.device);
+                const int rc = step_member(m, dt);
+                if (rc != OGX_OK) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if (rc_first == OGX_OK) {
+                        rc_first = rc;
+                        msg = g_last_error;
+                    }
+                }
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (std::thread& t : pool) t.join();
+        if (rc_first != OGX_OK) {
+            set_last_error(rc_first, msg);
+            return rc_first;
+        }
         ++e.member_steps;
         bool ready = true;
         for (Handle* h : e.members) ready = ready && h->step_exec && h->step_gen == h->ws.generation;
