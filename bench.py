@@ -191,11 +191,11 @@ def serve_run(args, timeout=600):
 def serving_records():
     """Config 4 (64 resident systems, N log-uniform 8k-256k, p in {6, 8}, 50 lockstep steps)
     and config 5 (24 jobs arriving at 20/s, N 16k-1M, p in {6, 8, 12}, 10-200 steps, 150 GB
-    budget) through the serving driver, mixed form, eager steps (a job's first steps would pay
-    for capturing its step, which these short jobs do not amortise);
-    config 4 also with every lockstep step as one graph launch, config 5 also as the plain
-    FP64 form run one job after another (the comparison config 5 names).  Seeded synthetic
-    jobs; wall-clock figures from the driver's own clock."""
+    budget) through the serving driver, mixed form: config 4 with eager steps on eight host
+    threads and with every lockstep step as one graph launch; config 5 with every job
+    replaying its captured step, and as the plain FP64 form run one job after another, eager
+    (the comparison config 5 names).  Seeded synthetic jobs; wall-clock figures from the
+    driver's own clock."""
     out = {}
     keep4 = ("bodies_steps_per_s", "steady_bodies_steps_per_s", "ensemble_step_ms_p50", "ensemble_step_ms_p99",
              "p50_step_ms", "p99_step_ms", "jobs", "failed", "rejected", "graph_launch_steps", "wall_s")
@@ -206,7 +206,7 @@ def serving_records():
         out["config4_ensemble_workers"] = {k: d.get(k) for k in keep4} if "failed" not in d or d["failed"] == 0 else d
         d = serve_run(CONFIG4 + ["--graph"])
         out["config4_ensemble_one_launch_per_step"] = {k: d.get(k) for k in keep4} if "failed" not in d or d["failed"] == 0 else d
-        d = serve_run(CONFIG5)
+        d = serve_run(CONFIG5 + ["--capture"])
         out["config5_served_mixed"] = {k: d.get(k) for k in keep5} if "failed" not in d or d["failed"] == 0 else d
         b = serve_run(CONFIG5 + ["--solo", "--precision", "fp64"], timeout=900)
         out["config5_fp64_sequential"] = {k: b.get(k) for k in keep5} if "failed" not in b or b["failed"] == 0 else b
