@@ -52,11 +52,14 @@ DT = 0.01
 M2L_DRAM_BYTES_PER_VPAIR = 15.82
 
 
-def arm_config(n, n_per, world):
+def arm_config(n, n_per, world, eps=0.0, softening="plummer"):
     """The workload this arm is quoted on."""
-    return {"workload": f"two-galaxy merger, {n} bodies (2x{n_per} disk+bulge), one leapfrog step dt=0.01",
-            "p": P_ORDER, "leaf_capacity": THR, "eps": 0.0, "parallelism": f"replicas x{world}",
-            "l2": "flushed (256 MiB write) before every timed step"}
+    cfg = {"workload": f"two-galaxy merger, {n} bodies (2x{n_per} disk+bulge), one leapfrog step dt=0.01",
+           "p": P_ORDER, "leaf_capacity": THR, "eps": eps, "parallelism": f"replicas x{world}",
+           "l2": "flushed (256 MiB write) before every timed step"}
+    if softening != "plummer":
+        cfg["softening"] = softening
+    return cfg
 
 
 def reference_config(nsys, n_sys, n_per_full, world):
@@ -98,6 +101,9 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-capture", action="store_true", help="eager steps instead of replaying a captured CUDA graph")
     ap.add_argument("--no-serving", action="store_true", help="skip the ensemble (config 4) and serving (config 5) records")
+    ap.add_argument("--eps", type=float, default=0.0, help="softening length of the timed workload (default 0)")
+    ap.add_argument("--softening", default="plummer", choices=["plummer", "spline"],
+                    help="softening kernel of the timed workload (spline: compact kernel, far field corrected)")
     return ap.parse_args()
 
 
@@ -323,7 +329,9 @@ def main():
     with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as ic_solver:
         pos, vel, mass, _ = ogx_ic.merger(args.n_per, seed=1, accel_fn=ic_solver.compute_accelerations)
     n = mass.shape[0]
-    solver = ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=prec, device=local, stream=stream.cuda_stream)
+    soft = ogx.SOFT_SPLINE if args.softening == "spline" else ogx.SOFT_PLUMMER
+    solver = ogx.AdaptiveFMM3D(eps=args.eps, p=P_ORDER, threshold=THR, precision=prec, device=local,
+                               stream=stream.cuda_stream, softening=soft)
     # each timed step replays a CUDA graph captured during the warm-up (no count read-back
     # in the middle of a step; a step that outgrows its capacities is redone eagerly)
     solver.set_tuning(capture_steps=0 if args.no_capture else 1)
@@ -382,9 +390,10 @@ def main():
     acc_info = {}
     if not args.no_accuracy and rank == 0:
         acc_form = acc_h.numpy().copy()
-        with ogx.DirectSolver3D(device=local) as d:
+        with ogx.DirectSolver3D(eps=args.eps, device=local, softening=soft) as d:
             ref = d.compute_accelerations(pos, mass)
-        with ogx.AdaptiveFMM3D(p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local) as f64:
+        with ogx.AdaptiveFMM3D(eps=args.eps, p=P_ORDER, threshold=THR, precision=ogx.PREC_FP64, device=local,
+                               softening=soft) as f64:
             acc64 = f64.compute_accelerations(pos, mass)
 
         rms, mx = rms_max(ref, acc_form)
@@ -397,7 +406,8 @@ def main():
     # the plain FP64 form at p = 8 (the mixed/plain speed-up), and both forms at p = 10,
     # the lowest order whose truncation error against the FP64 direct sum is below 1e-5
     forms = {}
-    if not args.no_accuracy and rank == 0 and prec == ogx.PREC_MIXED:
+    if (not args.no_accuracy and rank == 0 and prec == ogx.PREC_MIXED and args.eps == 0.0
+            and args.softening == "plummer"):
         nf = max(3, min(args.steps, 5))
         forms["fp64_p8"] = time_form(ogx, ogx.PREC_FP64, P_ORDER, pos, vel, mass, local, stream, flush, nf)
         forms["fp64_p8"]["mixed_speedup"] = forms["fp64_p8"]["ms_per_step"] / ms_per_step
@@ -450,7 +460,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "mixed(f32 P2P, scaled 3xFP16 tensor-core M2L, f64 translations)" if prec == ogx.PREC_MIXED else ("f64 (rotation-based M2L)" if prec == ogx.PREC_FP64_ROT else "f64"),
         "data": "synthetic",
-        "config": arm_config(n, args.n_per, world),
+        "config": arm_config(n, args.n_per, world, args.eps, args.softening),
         "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
         "e2e": {"value": replica_value(n, world, e2e_mean), "unit": "bodies/s", "h2d_bytes_per_step": int(32 * n),
                 "d2h_bytes_per_step": int(24 * n), "ms_per_step": e2e_mean},
