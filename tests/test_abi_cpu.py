@@ -129,3 +129,20 @@ def test_rotation_factors_multiply_back_to_the_m2l_matrix(ogx, p):
         # each row's entries against that row's scale (rows of high degree are small)
         scale = np.abs(T).max(axis=1, keepdims=True)
         assert np.max(np.abs(R - T) / scale) <= 1e-13, (p, idx)
+
+
+def test_python_params_struct_covers_the_c_struct(ogx):
+    """ogx_params_default fills the whole C struct: the binding's mirror must be at least as
+    large (a canary behind it must stay intact) and read back the documented defaults."""
+    import ctypes as C
+
+    class Guarded(C.Structure):
+        _fields_ = [("prm", ogx.Params), ("canary", C.c_uint64 * 4)]
+
+    g = Guarded()
+    for i in range(4):
+        g.canary[i] = 0x5A5A5A5A5A5A5A5A
+    assert ogx.load().ogx_params_default(C.byref(g.prm)) == 0
+    assert all(g.canary[i] == 0x5A5A5A5A5A5A5A5A for i in range(4))
+    assert (g.prm.G, g.prm.eps, g.prm.p, g.prm.leaf_capacity) == (1.0, 0.0, 8, 64)
+    assert g.prm.softening == ogx.SOFT_PLUMMER
