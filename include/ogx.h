@@ -180,11 +180,13 @@ typedef struct {
 } ogx_tuning;
 int ogx_set_tuning(void* handle, const ogx_tuning* t);
 int ogx_get_tuning(void* handle, ogx_tuning* out);
-/* Diagnostic with no counterpart in the reference: runs the bounded device wait of the
- * tensor-core M2L pipeline (an mbarrier wait that gives up after a poll limit and sets the
- * handle's device error word) on a barrier that nothing arrives on, with `polls` (>= 1) as the
- * limit.  Returns OGX_ERR_TIMEOUT, as an evaluation whose pipeline wait ran out does, and
- * leaves the handle usable: the error word is cleared when it is reported. */
+/* Diagnostic with no counterpart in the reference: runs the library's two kinds of bounded
+ * device wait, each giving up after a poll limit and setting the handle's device error word,
+ * on something that never happens, with `polls` (>= 1) as the limit: the tensor-core M2L
+ * pipeline's mbarrier wait on a barrier nothing arrives on, and the translation passes' wait
+ * on a box's ready flag that nothing sets.  Returns OGX_ERR_TIMEOUT when both ran out, as an
+ * evaluation whose wait ran out does, and leaves the handle usable: the error word is
+ * cleared when it is reported. */
 int ogx_check_bounded_wait(void* handle, uint32_t polls);
 /* Text of the last error raised on the calling host thread (CUDA message etc.). */
 const char* ogx_last_error_message(void);

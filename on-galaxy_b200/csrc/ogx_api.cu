@@ -1160,13 +1160,30 @@ int ogx_check_bounded_wait(void* handle, uint32_t polls) {
     DevCounts* dc;
     OGX_TRY(arena_get(h.ws, S_COUNTS, 1, &dc));
     h.d_err = &dc->kernel_error;
-    OGX_CUDA(cudaMemsetAsync(h.d_err, 0, sizeof(int), h.stream));
-    k_wait_probe<<<1, 32, 0, h.stream>>>(polls, h.d_err);
-    ++h.launches;
-    OGX_CUDA(cudaGetLastError());
-    OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    int ran_out[2] = {0, 0};
+    for (int k = 0; k < 2; ++k) {
+        // the error word and, for the flag wait, a flag nothing sets (the word beside it)
+        OGX_CUDA(cudaMemsetAsync(h.d_err, 0, 2 * sizeof(int), h.stream));
+        if (k == 0) {   // the tensor-core pipeline's mbarrier wait
+            k_wait_probe<<<1, 32, 0, h.stream>>>(polls, h.d_err);
+            ++h.launches;
+            OGX_CUDA(cudaGetLastError());
+        } else {        // the translation passes' wait on a box's ready flag
+            OGX_TRY(flag_wait_probe(h, polls, &dc->pad_err, h.d_err));
+        }
+        OGX_CUDA(cudaMemcpyAsync(h.h_err, h.d_err, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+        OGX_CUDA(cudaStreamSynchronize(h.stream));
+        ran_out[k] = *h.h_err;
+        *h.h_err = 0;
+    }
+    OGX_CUDA(cudaMemsetAsync(h.d_err, 0, 2 * sizeof(int), h.stream));
     OGX_CUDA(cudaStreamSynchronize(h.stream));
-    return device_error(h);
+    if (ran_out[0] && ran_out[1]) {
+        set_last_error(OGX_ERR_TIMEOUT, "both bounded device waits ran out (mbarrier and ready flag)");
+        return OGX_ERR_TIMEOUT;
+    }
+    set_last_error(OGX_ERR_STATE, "a bounded device wait given nothing to wait for did not run out");
+    return OGX_ERR_STATE;
 }
 
 }  // extern "C"

@@ -130,8 +130,8 @@ __device__ __forceinline__ void st_release_gpu(int* p, int v) {
 }
 // bounded wait until *flag != 0; false when it ran out (*err is then set) or when
 // another wait already gave up
-__device__ bool wait_ready(const int* flag, int* err) {
-    for (uint32_t it = 0; it < sm100::kSpinLimit; ++it) {
+__device__ bool wait_ready(const int* flag, int* err, uint32_t limit = sm100::kSpinLimit) {
+    for (uint32_t it = 0; it < limit; ++it) {
         if (ld_acquire_gpu(flag)) return true;
         if (*(volatile int*)err) return false;
         if (it > 16) __nanosleep(64);
@@ -565,6 +565,19 @@ __global__ void __launch_bounds__(128) k_soft_correct(TreeView tv, const int64_t
 }
 
 }  // namespace
+
+// One thread runs the translation passes' bounded flag wait, with a limit of `polls`, on
+// a flag that nothing sets: the wait runs out and sets *err as in the passes.
+__global__ void k_flag_wait_probe(const int* flag, int* err, uint32_t polls) {
+    if (threadIdx.x == 0) wait_ready(flag, err, polls);
+}
+
+int flag_wait_probe(Handle& h, uint32_t polls, const int* flag, int* err) {
+    k_flag_wait_probe<<<1, 32, 0, h.stream>>>(flag, err, polls);
+    ++h.launches;
+    OGX_CUDA(cudaGetLastError());
+    return OGX_OK;
+}
 
 // work items of the near field (leaf, chunk of 32 targets), on h.stream; the grid of a
 // warp-per-item kernel needs at most nleaf + n / 32 warps

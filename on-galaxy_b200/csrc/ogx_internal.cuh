@@ -155,7 +155,7 @@ struct DevCounts {
     int64_t adj_mismatch;
     int64_t v_total;
     int32_t kernel_error;  // set by kernels whose bounded waits ran out
-    int32_t pad_err;
+    int32_t pad_err;       // zero: the bounded-wait probe's flag that nothing sets
     int32_t nonleaf_level[kMaxDepth + 2];
     int32_t deep_flag;   // some level-16 box holds more than leaf_capacity bodies
     int32_t overflow;    // capacity mode: a count above its capacity (see above)
@@ -340,6 +340,7 @@ int fmm_mixed(Handle& h, double* d_acc, double* d_pot);
 int m2l_rot_launch(Handle& h, const double* M, double* Lown);   // third form's M2L, on h.stream
 int fmm_mixed_upward(Handle& h);   // upward pass on h.up, right after the tree (before the lists)
 int fmm_mixed_m2l(Handle& h, bool pot);   // tensor-core M2L on h.m2l, after the target tiles
+int flag_wait_probe(Handle& h, uint32_t polls, const int* flag, int* err);   // translation passes' wait, run out
 int direct_eval(Handle& h, const double* d_pos, const double* d_mass, int64_t n, double* d_acc,
                 double* d_pot, bool fp32);
 int ensure_operator_tables(Handle& h);

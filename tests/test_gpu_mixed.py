@@ -69,7 +69,8 @@ def test_mixed_leapfrog_runs_and_tracks_fp64(ogx, golden):
 
 def test_bounded_wait_runs_out_and_the_handle_stays_usable(ogx, golden):
     """The tensor-core pipeline's bounded mbarrier wait, given a barrier nothing arrives on,
-    gives up after its poll limit and the host reports OGX_ERR_TIMEOUT (no copy or MMA is
+    and the translation passes' bounded ready-flag wait, given a flag nothing sets, both give
+    up after their poll limit and the host reports OGX_ERR_TIMEOUT (no copy or MMA is
     outstanding, so no GPU fault is involved); the same handle then evaluates as before."""
     d = golden("plummer2000_s2")
     with ogx.AdaptiveFMM3D(p=8, threshold=64, precision=ogx.PREC_MIXED) as s:
