@@ -111,6 +111,20 @@ def test_softened_jobs_give_the_same_bits_alone_and_in_the_mix():
     assert all(a != b for a, b in zip(digests, [j["digest"] for j in plummer["jobs_detail"]]))
 
 
+@pytest.mark.gpu
+def test_softened_ensemble_members_match_their_solo_runs():
+    """Spline-softened systems step eagerly (their steps are never captured), so with --graph
+    every lockstep step runs the members on the ensemble's host threads; each member still
+    ends bit-identical to its solo run."""
+    args = ("--ensemble", "--steps", 3, "--jobs", 10, "--nmin", 8192, "--nmax", 65536, "--orders", "6,8",
+            "--seed", 17, "--eps", 0.05, "--softening", "spline")
+    ens = _serve(*args, "--graph")
+    solo = _serve(*args, "--solo")
+    assert ens["failed"] == 0 and solo["failed"] == 0
+    assert ens["graph_launch_steps"] == 0 and ens["member_by_member_steps"] == 3
+    assert [j["digest"] for j in ens["jobs_detail"]] == [j["digest"] for j in solo["jobs_detail"]]
+
+
 def test_serve_rejects_an_unknown_softening():
     if not os.path.exists(SERVE):
         pytest.skip("ogx_serve not built")
